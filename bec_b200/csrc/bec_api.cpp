@@ -1,0 +1,1222 @@
+// bec_api.cpp -- host side of the engine: the C ABI of include/bec.h.
+//
+// Replaces the reference's host driver (programs/bec_wigner_3d.cuda/wigner.cu,
+// wigner.cpp:119-176, defines.h:115-210): parameter derivation, device
+// buffers, the ground-state loop, ensemble initialisation, the split-step
+// loop and the observables. All state lives in a bec_ctx; errors return
+// status codes; host arrays belong to the caller.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace {
+
+const double kHbar = 1.054571628e-34;   // wigner.cpp:121
+const double kBohr = 5.2917720859e-11;  // wigner.cpp:122
+
+// Neumaier-compensated host accumulator
+struct HSum {
+    double s = 0.0, c = 0.0;
+    void add(double v)
+    {
+        double t = s + v;
+        if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v; else c += (v - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+int ilog2(int n) { int r = 0; while ((1 << r) < n) ++r; return r; }
+
+struct GroupRec {
+    bec_params p;
+    bec_derived d;
+    GeomD gd;
+    GroupParamsF gf;
+    int cls = -1;             // grid class (batched path)
+    int traj_first = 0;       // global trajectory index of the first trajectory
+    int local_first = 0;      // index within the class
+    double2 *a = nullptr, *b = nullptr;   // plain path: k-space state [ne][cells]
+    double2 *gs_dev = nullptr;            // batched path: x-space ground state
+    bool initialised = false;
+};
+
+struct ClassRec {
+    ClassGeom geom{};
+    float4 *state = nullptr;
+    int *d_tgroup = nullptr, *d_tlocal = nullptr;
+    double *d_traj_scale = nullptr;
+    double *obs_partial = nullptr;
+    double *traj_axial = nullptr;
+    int tiles = 1;
+    int traj_offset = 0;      // global index of the class's first trajectory
+    std::vector<int> groups;  // group indices in this class
+};
+
+} // namespace
+
+struct bec_ctx {
+    int path = 0;
+    int n_traj = 0;
+    std::vector<GroupRec> groups;
+    std::vector<ClassRec> classes;
+    std::map<int, double2 *> tw64;
+    std::map<int, float2 *> tw32;
+    GroupParamsF *d_gparams = nullptr;
+    double *d_traj_tot = nullptr;        // [n_traj][4]
+    double *d_group_mom = nullptr;       // [n_groups][4]
+    int *d_group_first = nullptr, *d_group_count = nullptr;
+    double *d_red = nullptr;             // reduction scratch
+    double *d_scal = nullptr;            // device scalars
+    double *d_plain_obs = nullptr;       // plain path per-trajectory per-z sums [n_traj][nzmax][4]
+    double *d_plain_axial = nullptr;     // [n_traj][nzmax][4]
+    double2 *scratch_a = nullptr, *scratch_b = nullptr;  // plain: x-space copies (max cells)
+    float4 *scratch4 = nullptr;          // batched: one trajectory (max cells)
+    int max_cells = 0, max_nz = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    long long step = 0;         // steps since initialisation (Philox counter)
+    long long evo_steps = 0;    // steps since bec_start_evolution
+    bool pending = false;       // batched: last step's second half-kick not yet applied
+    bool has_pulse = false;     // batched: pulse waiting for the next z pass
+    double2 pulse[4];           // pending pulse matrix (row-major)
+    double last_ms = 0.0;
+    long long last_launches = 0;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+bec_status fail(bec_ctx *c, bec_status st, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return st;
+}
+
+#define CKC(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? BEC_ERR_OUT_OF_MEMORY : BEC_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+    } while (0)
+
+#define CKL()                                                                                       \
+    do {                                                                                            \
+        cudaError_t e_ = cudaGetLastError();                                                        \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(ctx, BEC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(bec_ctx *ctx, T **p, size_t n)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+    if (e == cudaSuccess) {
+        ctx->allocs.push_back(q);
+        *p = static_cast<T *>(q);
+    }
+    return e;
+}
+
+double2 cd(double re, double im) { return make_double2(re, im); }
+
+// report.tex rotation matrix: [[cos t/2, -i e^{-i phi} sin t/2], [-i e^{i phi} sin t/2, cos t/2]]
+void rotation(double theta, double phi, double2 m[4])
+{
+    const double c = std::cos(theta / 2.0), s = std::sin(theta / 2.0);
+    m[0] = cd(c, 0.0);
+    m[1] = cd(-s * std::sin(phi), -s * std::cos(phi));   // -i e^{-i phi} s
+    m[2] = cd(s * std::sin(phi), -s * std::cos(phi));    // -i e^{+i phi} s
+    m[3] = cd(c, 0.0);
+}
+
+void matmul2(const double2 a[4], const double2 b[4], double2 out[4])
+{
+    auto mul = [](double2 x, double2 y) { return cd(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x); };
+    auto add = [](double2 x, double2 y) { return cd(x.x + y.x, x.y + y.y); };
+    double2 r[4];
+    r[0] = add(mul(a[0], b[0]), mul(a[1], b[2]));
+    r[1] = add(mul(a[0], b[1]), mul(a[1], b[3]));
+    r[2] = add(mul(a[2], b[0]), mul(a[3], b[2]));
+    r[3] = add(mul(a[2], b[1]), mul(a[3], b[3]));
+    for (int i = 0; i < 4; ++i) out[i] = r[i];
+}
+
+GeomD make_geomd(const bec_params &p, const bec_derived &d)
+{
+    GeomD g{};
+    g.nx = d.nvx; g.ny = d.nvy; g.nz = d.nvz;
+    g.lx = ilog2(d.nvx); g.ly = ilog2(d.nvy); g.lz = ilog2(d.nvz);
+    g.cells = d.cells;
+    g.dkx = d.dkx; g.dky = d.dky; g.dkz = d.dkz;
+    g.xmax = d.xmax; g.ymax = d.ymax; g.zmax = d.zmax;
+    g.dx = d.dx; g.dy = d.dy; g.dz = d.dz; g.lambda = d.lambda;
+    g.g11 = d.g11; g.g12 = d.g12; g.g22 = d.g22;
+    g.l111 = d.l111; g.l12 = d.l12; g.l22 = d.l22; g.detuning = d.detuning;
+    g.dt_evo = d.dt_evo; g.dt_steady = d.dt_steady; g.dV = d.dV;
+    g.Va = d.Va; g.Vb = d.Vb;
+    g.itmax = d.itmax;
+    g.noise = (p.loss_noise && (d.l111 > 0 || d.l12 > 0 || d.l22 > 0)) ? 1 : 0;
+    g.seed = p.seed;
+    return g;
+}
+
+GroupParamsF make_gf(const GeomD &g)
+{
+    GroupParamsF f{};
+    f.dkx = (float)g.dkx; f.dky = (float)g.dky; f.dkz = (float)g.dkz;
+    f.xmax = (float)g.xmax; f.ymax = (float)g.ymax; f.zmax = (float)g.zmax;
+    f.dx = (float)g.dx; f.dy = (float)g.dy; f.dz = (float)g.dz;
+    f.inv_lambda2 = (float)(1.0 / (g.lambda * g.lambda));
+    f.g11 = (float)g.g11; f.g12 = (float)g.g12; f.g22 = (float)g.g22;
+    f.l111 = (float)g.l111; f.l12 = (float)g.l12; f.l22 = (float)g.l22;
+    f.detuning = (float)g.detuning;
+    f.dt = (float)g.dt_evo;
+    f.noise_amp = (float)std::sqrt(g.dt_evo / (2.0 * g.dV));
+    f.c1 = (float)(std::sqrt(g.l111 / 6.0) * 3.0);
+    f.c2 = (float)std::sqrt(g.l12 / 2.0);
+    f.c3 = (float)std::sqrt(g.l22);
+    f.init_a = (float)(g.Va / std::sqrt(g.dV));
+    f.init_b = (float)(g.Vb / std::sqrt(g.dV));
+    f.itmax = g.itmax;
+    f.noise = g.noise;
+    f.seed_lo = (uint32_t)g.seed;
+    f.seed_hi = (uint32_t)(g.seed >> 32);
+    return f;
+}
+
+// W_n^k = exp(-2 pi i k / n), k < n/2, in double
+std::vector<double2> twiddles(int n)
+{
+    std::vector<double2> t(n / 2 > 0 ? n / 2 : 1);
+    for (int k = 0; k < n / 2; ++k) {
+        double a = 2.0 * M_PI * (double)k / (double)n;
+        t[k] = cd(std::cos(a), -std::sin(a));
+    }
+    if (n / 2 == 0) t[0] = cd(1.0, 0.0);
+    return t;
+}
+
+bec_status get_tw64(bec_ctx *ctx, int n, double2 **out)
+{
+    auto it = ctx->tw64.find(n);
+    if (it != ctx->tw64.end()) { *out = it->second; return BEC_OK; }
+    std::vector<double2> t = twiddles(n);
+    double2 *d = nullptr;
+    CKC(dalloc(ctx, &d, t.size()));
+    CKC(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    ctx->tw64[n] = d;
+    *out = d;
+    return BEC_OK;
+}
+
+bec_status get_tw32(bec_ctx *ctx, int n, float2 **out)
+{
+    auto it = ctx->tw32.find(n);
+    if (it != ctx->tw32.end()) { *out = it->second; return BEC_OK; }
+    std::vector<double2> t = twiddles(n);
+    std::vector<float2> f(t.size());
+    for (size_t i = 0; i < t.size(); ++i) f[i] = make_float2((float)t[i].x, (float)t[i].y);
+    float2 *d = nullptr;
+    CKC(dalloc(ctx, &d, f.size()));
+    CKC(cudaMemcpy(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    ctx->tw32[n] = d;
+    *out = d;
+    return BEC_OK;
+}
+
+bec_status plain_fft(bec_ctx *ctx, double2 *data, const GeomD &g, int inv)
+{
+    double2 *tx, *ty, *tz;
+    bec_status st;
+    if ((st = get_tw64(ctx, g.nx, &tx))) return st;
+    if ((st = get_tw64(ctx, g.ny, &ty))) return st;
+    if ((st = get_tw64(ctx, g.nz, &tz))) return st;
+    plain_fft3d(data, g, tx, ty, tz, inv, ctx->stream);
+    return BEC_OK;
+}
+
+// ---------------------------------------------------------------- plain step
+// propagate (wigner.cu:178-199) for one trajectory
+bec_status plain_step(bec_ctx *ctx, GroupRec &gr, int t)
+{
+    const GeomD &g = gr.gd;
+    double2 *a = gr.a + (size_t)t * g.cells, *b = gr.b + (size_t)t * g.cells;
+    bec_status st;
+    plain_kick(a, b, g, 1.0, 0, ctx->stream);
+    if ((st = plain_fft(ctx, a, g, 0))) return st;
+    if ((st = plain_fft(ctx, b, g, 0))) return st;
+    plain_nl(a, b, g, (uint32_t)t, (uint32_t)ctx->step, ctx->stream);
+    if ((st = plain_fft(ctx, a, g, 1))) return st;
+    if ((st = plain_fft(ctx, b, g, 1))) return st;
+    plain_kick(a, b, g, 1.0 / g.cells, 1, ctx->stream);
+    return BEC_OK;
+}
+
+// ---------------------------------------------------------------- batched z pass
+// ends_step: no plane pass follows, so the pass leaves the state in the form a z pass reads
+bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, const double2 *m2,
+                             bool ends_step = false)
+{
+    ZPassArgs z{};
+    z.pre = pre;
+    z.post = post;
+    z.observe = observe ? 1 : 0;
+    if (ctx->has_pulse) {
+        z.has_m1 = 1;
+        for (int i = 0; i < 4; ++i) z.m1[i] = make_float2((float)ctx->pulse[i].x, (float)ctx->pulse[i].y);
+    }
+    if (m2) {
+        z.has_m2 = 1;
+        for (int i = 0; i < 4; ++i) z.m2[i] = make_float2((float)m2[i].x, (float)m2[i].y);
+    }
+    for (auto &c : ctx->classes) {
+        if (c.geom.n_traj == 0) continue;
+        float2 *tz;
+        bec_status st;
+        if ((st = get_tw32(ctx, c.geom.nz, &tz))) return st;
+        z.scale = (float)(1.0 / (double)c.geom.cells);
+        z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
+        fp32_zpass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, tz, z, c.obs_partial, ctx->stream);
+        CKL();
+    }
+    ctx->has_pulse = false;
+    return BEC_OK;
+}
+
+bec_status batched_ppass_all(bec_ctx *ctx)
+{
+    for (auto &c : ctx->classes) {
+        if (c.geom.n_traj == 0) continue;
+        float2 *tx, *ty;
+        bec_status st;
+        if ((st = get_tw32(ctx, c.geom.nx, &tx))) return st;
+        if ((st = get_tw32(ctx, c.geom.ny, &ty))) return st;
+        fp32_ppass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, tx, ty, (uint32_t)ctx->step,
+                   ctx->stream);
+        CKL();
+    }
+    return BEC_OK;
+}
+
+// reduces the partial sums of the last observing z pass into d_traj_tot / axial / group moments
+bec_status batched_reduce_obs(bec_ctx *ctx)
+{
+    for (auto &c : ctx->classes) {
+        if (c.geom.n_traj == 0) continue;
+        obs_reduce(c.obs_partial, c.geom.n_traj, c.tiles, c.geom.nz, c.d_traj_scale, c.traj_axial,
+                   ctx->d_traj_tot + (size_t)c.traj_offset * 4, ctx->stream);
+        CKL();
+    }
+    group_reduce(ctx->d_traj_tot, ctx->d_group_first, ctx->d_group_count, (int)ctx->groups.size(),
+                 ctx->d_group_mom, ctx->stream);
+    CKL();
+    return BEC_OK;
+}
+
+// Brings the batched state to a step boundary with no pending kick or pulse.
+bec_status batched_resolve(bec_ctx *ctx, bool observe)
+{
+    if (!ctx->pending && !ctx->has_pulse && !observe) return BEC_OK;
+    bec_status st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.0f, observe, nullptr, true);
+    if (st) return st;
+    ctx->pending = false;
+    return BEC_OK;
+}
+
+// plain path: per-trajectory per-z sums of x-space copies, then reductions
+bec_status plain_observe(bec_ctx *ctx)
+{
+    CKC(cudaMemsetAsync(ctx->d_plain_obs, 0, sizeof(double) * (size_t)ctx->n_traj * ctx->max_nz * 4, ctx->stream));
+    for (auto &gr : ctx->groups) {
+        const GeomD &g = gr.gd;
+        for (int t = 0; t < gr.p.ne; ++t) {
+            CKC(cudaMemcpyAsync(ctx->scratch_a, gr.a + (size_t)t * g.cells, sizeof(double2) * g.cells,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+            CKC(cudaMemcpyAsync(ctx->scratch_b, gr.b + (size_t)t * g.cells, sizeof(double2) * g.cells,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+            bec_status st;
+            if ((st = plain_fft(ctx, ctx->scratch_a, g, 0))) return st;
+            if ((st = plain_fft(ctx, ctx->scratch_b, g, 0))) return st;
+            plain_axial_sums(ctx->scratch_a, ctx->scratch_b, g,
+                             ctx->d_plain_obs + (size_t)(gr.traj_first + t) * ctx->max_nz * 4, ctx->stream);
+            CKL();
+        }
+    }
+    // the per-trajectory rows are max_nz long; groups with a shorter nz have zero tails
+    obs_reduce(ctx->d_plain_obs, ctx->n_traj, 1, ctx->max_nz, nullptr, ctx->d_plain_axial, ctx->d_traj_tot,
+               ctx->stream);
+    CKL();
+    group_reduce(ctx->d_traj_tot, ctx->d_group_first, ctx->d_group_count, (int)ctx->groups.size(),
+                 ctx->d_group_mom, ctx->stream);
+    CKL();
+    return BEC_OK;
+}
+
+bec_status check_ready(bec_ctx *ctx)
+{
+    for (auto &g : ctx->groups)
+        if (!g.initialised) return fail(ctx, BEC_ERR_STATE, "every group needs bec_init_group first");
+    return BEC_OK;
+}
+
+bec_status do_evolve(bec_ctx *ctx, int n)
+{
+    bec_status st;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        for (int s = 0; s < n; ++s) {
+            for (auto &gr : ctx->groups)
+                for (int t = 0; t < gr.p.ne; ++t)
+                    if ((st = plain_step(ctx, gr, t))) return st;
+            CKL();
+            ctx->step++;
+            ctx->evo_steps++;
+        }
+    } else {
+        for (int s = 0; s < n; ++s) {
+            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
+            ctx->pending = true;
+            if ((st = batched_ppass_all(ctx))) return st;
+            ctx->step++;
+            ctx->evo_steps++;
+        }
+    }
+    return BEC_OK;
+}
+
+bec_status apply_pulse(bec_ctx *ctx, const double2 m[4])
+{
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        for (auto &gr : ctx->groups) {
+            plain_pulse(gr.a, gr.b, gr.p.ne * gr.gd.cells, m[0], m[1], m[2], m[3], ctx->stream);
+            CKL();
+        }
+    } else {
+        if (ctx->has_pulse) {
+            double2 r[4];
+            matmul2(m, ctx->pulse, r);
+            for (int i = 0; i < 4; ++i) ctx->pulse[i] = r[i];
+        } else {
+            for (int i = 0; i < 4; ++i) ctx->pulse[i] = m[i];
+        }
+        ctx->has_pulse = true;
+    }
+    return BEC_OK;
+}
+
+bec_status fetch_group_moments(bec_ctx *ctx, bec_moments *out)
+{
+    const size_t ng = ctx->groups.size();
+    std::vector<double> h(ng * 4);
+    CKC(cudaMemcpyAsync(h.data(), ctx->d_group_mom, sizeof(double) * ng * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CKC(cudaStreamSynchronize(ctx->stream));
+    for (size_t g = 0; g < ng; ++g) {
+        out[g].t = ctx->evo_steps * ctx->groups[g].p.dt_evo;
+        out[g].na = h[g * 4 + 0];
+        out[g].nb = h[g * 4 + 1];
+        out[g].s_re = h[g * 4 + 2];
+        out[g].s_im = h[g * 4 + 3];
+        if (!std::isfinite(out[g].na) || !std::isfinite(out[g].nb) || !std::isfinite(out[g].s_re) ||
+            !std::isfinite(out[g].s_im))
+            return fail(ctx, BEC_ERR_NUMERICAL, "non-finite moments (state diverged)");
+    }
+    return BEC_OK;
+}
+
+bec_status observe_now(bec_ctx *ctx)
+{
+    if (ctx->path == BEC_PATH_FP64_PLAIN) return plain_observe(ctx);
+    bec_status st = batched_resolve(ctx, true);
+    if (st) return st;
+    return batched_reduce_obs(ctx);
+}
+
+} // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+int32_t bec_abi_version(void) { return BEC_ABI_VERSION; }
+
+bec_status bec_derive_params(const bec_params *p, bec_derived *d)
+{
+    if (!p || !d) return BEC_ERR_INVALID_ARG;
+    if (!is_pow2(p->nvx) || !is_pow2(p->nvy) || !is_pow2(p->nvz) || p->nvx < 2 || p->nvz < 2)
+        return BEC_ERR_UNSUPPORTED_GRID;
+    if (!(p->m > 0) || !(p->fx > 0) || !(p->fz > 0) || !(p->N > 0) || p->ne < 1 || p->itmax < 1)
+        return BEC_ERR_INVALID_ARG;
+    std::memset(d, 0, sizeof(*d));
+    const double w_rho = 2.0 * M_PI * p->fx;
+    d->l_rho = std::sqrt(kHbar / (p->m * w_rho));
+    d->t_rho = 1.0 / w_rho;
+    d->lambda = p->fx / p->fz;
+    d->nvx = p->nvx; d->nvy = p->nvy; d->nvz = p->nvz;
+    d->cells = p->nvx * p->nvy * p->nvz;
+    d->dims = (p->nvy == 1) ? 2 : 3;
+    d->Va = p->Va; d->Vb = p->Vb;
+    d->V = (p->Va + p->Vb) / 2.0;
+    d->detuning = 2.0 * M_PI * p->detuning / w_rho;
+    d->l111 = p->gamma111 / (std::pow(d->l_rho, 6) * w_rho);
+    d->l12 = p->gamma12 / (std::pow(d->l_rho, 3) * w_rho);
+    d->l22 = p->gamma22 / (std::pow(d->l_rho, 3) * w_rho);
+    d->g11 = 4.0 * M_PI * p->a11 * kBohr / d->l_rho;
+    d->g12 = 4.0 * M_PI * p->a12 * kBohr / d->l_rho;
+    d->g22 = 4.0 * M_PI * p->a22 * kBohr / d->l_rho;
+    d->N = p->N;
+    if (d->dims == 3) {
+        d->mu = std::pow(15.0 * d->N * d->g11 / (16.0 * M_PI * d->lambda * std::sqrt(2.0)), 0.4);
+        d->xmax = 1.2 * std::sqrt(2.0 * d->mu);
+        d->ymax = 1.2 * std::sqrt(2.0 * d->mu);
+        d->zmax = 1.2 * d->lambda * std::sqrt(2.0 * d->mu);
+        d->dx = 2.0 * d->xmax / (d->nvx - 1);
+        d->dy = 2.0 * d->ymax / (d->nvy - 1);
+        d->dz = 2.0 * d->zmax / (d->nvz - 1);
+        d->dkx = M_PI / d->xmax;
+        d->dky = M_PI / d->ymax;
+        d->dkz = M_PI / d->zmax;
+    } else {
+        // 2D x-z slice: transverse oscillator ground state of width l_y = sqrt(hbar / m w_y);
+        // couplings and two-body rates scale by 1/(sqrt(2 pi) l_y), the three-body rate by
+        // 1/(sqrt(3) pi l_y^2); Thomas-Fermi N = pi lambda mu^2 / g11.
+        const double ly = std::sqrt(p->fx / (p->fy > 0 ? p->fy : p->fx));
+        const double s2 = 1.0 / (std::sqrt(2.0 * M_PI) * ly);
+        const double s3 = 1.0 / (std::sqrt(3.0) * M_PI * ly * ly);
+        d->g11 *= s2; d->g12 *= s2; d->g22 *= s2;
+        d->l12 *= s2; d->l22 *= s2; d->l111 *= s3;
+        d->mu = std::sqrt(d->N * d->g11 / (M_PI * d->lambda));
+        d->xmax = 1.2 * std::sqrt(2.0 * d->mu);
+        d->ymax = 0.0;
+        d->zmax = 1.2 * d->lambda * std::sqrt(2.0 * d->mu);
+        d->dx = 2.0 * d->xmax / (d->nvx - 1);
+        d->dy = 1.0;
+        d->dz = 2.0 * d->zmax / (d->nvz - 1);
+        d->dkx = M_PI / d->xmax;
+        d->dky = 0.0;
+        d->dkz = M_PI / d->zmax;
+    }
+    d->dV = d->dx * d->dy * d->dz;
+    d->itmax = p->itmax;
+    d->dt_steady = p->dt_steady / d->t_rho;
+    d->t_equilib = p->t_equilib / d->t_rho;
+    d->dt_evo = p->dt_evo / d->t_rho;
+    d->ne = p->ne;
+    int n = 0;
+    double t = 0.0;
+    if (d->dt_evo > 0) {
+        while (t <= d->t_equilib && n < 100000000) { ++n; t += d->dt_evo; }
+    } else {
+        n = 1;
+    }
+    d->n_equil_steps = n;
+    return BEC_OK;
+}
+
+bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, bec_ctx **out)
+{
+    if (!out) return BEC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!groups || n_groups < 1) return BEC_ERR_INVALID_ARG;
+    if (path != BEC_PATH_FP64_PLAIN && path != BEC_PATH_FP32_BATCHED) return BEC_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return BEC_ERR_NO_DEVICE;
+    }
+    bec_ctx *ctx = new bec_ctx();
+    ctx->path = path;
+    ctx->groups.resize(n_groups);
+    for (int g = 0; g < n_groups; ++g) {
+        GroupRec &gr = ctx->groups[g];
+        gr.p = groups[g];
+        bec_status st = bec_derive_params(&gr.p, &gr.d);
+        if (st) { delete ctx; return st; }
+        if (gr.d.nvx > 1024 || gr.d.nvy > 1024 || gr.d.nvz > 1024) { delete ctx; return BEC_ERR_UNSUPPORTED_GRID; }
+        if (path == BEC_PATH_FP32_BATCHED) {
+            // the z pass holds whole pencils of 16 (or nvx) columns; the plane pass whole planes
+            if (gr.d.nvz > 512 || gr.d.nvx * gr.d.nvy > 2048 || gr.d.nvz < 2) { delete ctx; return BEC_ERR_UNSUPPORTED_GRID; }
+        }
+        gr.gd = make_geomd(gr.p, gr.d);
+        gr.gf = make_gf(gr.gd);
+        ctx->max_cells = std::max(ctx->max_cells, gr.d.cells);
+        ctx->max_nz = std::max(ctx->max_nz, gr.d.nvz);
+    }
+    bec_status st = BEC_OK;
+    auto bail = [&](bec_status s) { bec_destroy(ctx); return s; };
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BEC_ERR_CUDA);
+    cudaEventCreate(&ctx->ev0);
+    cudaEventCreate(&ctx->ev1);
+
+    // trajectory numbering: classes in first-appearance order, groups in order within a class
+    if (path == BEC_PATH_FP32_BATCHED) {
+        for (int g = 0; g < n_groups; ++g) {
+            GroupRec &gr = ctx->groups[g];
+            int cls = -1;
+            for (size_t c = 0; c < ctx->classes.size(); ++c) {
+                const ClassGeom &cg = ctx->classes[c].geom;
+                if (cg.nx == gr.d.nvx && cg.ny == gr.d.nvy && cg.nz == gr.d.nvz) { cls = (int)c; break; }
+            }
+            if (cls < 0) {
+                ClassRec cr;
+                cr.geom.nx = gr.d.nvx; cr.geom.ny = gr.d.nvy; cr.geom.nz = gr.d.nvz;
+                cr.geom.lx = ilog2(gr.d.nvx); cr.geom.ly = ilog2(gr.d.nvy); cr.geom.lz = ilog2(gr.d.nvz);
+                cr.geom.cells = gr.d.cells;
+                cr.geom.n_traj = 0;
+                ctx->classes.push_back(cr);
+                cls = (int)ctx->classes.size() - 1;
+            }
+            gr.cls = cls;
+            ctx->classes[cls].groups.push_back(g);
+        }
+        int off = 0;
+        for (auto &c : ctx->classes) {
+            c.traj_offset = off;
+            int local = 0;
+            for (int g : c.groups) {
+                GroupRec &gr = ctx->groups[g];
+                gr.traj_first = off + local;
+                gr.local_first = local;
+                local += gr.p.ne;
+            }
+            c.geom.n_traj = local;
+            off += local;
+        }
+        ctx->n_traj = off;
+    } else {
+        int off = 0;
+        for (auto &gr : ctx->groups) { gr.traj_first = off; off += gr.p.ne; }
+        ctx->n_traj = off;
+    }
+    ctx->last_launches = 0;
+
+    // device buffers
+#define CKA(call) do { if ((call) != cudaSuccess) { cudaGetLastError(); return bail(BEC_ERR_OUT_OF_MEMORY); } } while (0)
+    const int ng = n_groups;
+    CKA(dalloc(ctx, &ctx->d_traj_tot, (size_t)ctx->n_traj * 4));
+    CKA(dalloc(ctx, &ctx->d_group_mom, (size_t)ng * 4));
+    CKA(dalloc(ctx, &ctx->d_group_first, (size_t)ng));
+    CKA(dalloc(ctx, &ctx->d_group_count, (size_t)ng));
+    CKA(dalloc(ctx, &ctx->d_red, (size_t)2 * 8 * 1024));
+    CKA(dalloc(ctx, &ctx->d_scal, (size_t)64));
+    {
+        std::vector<int> first(ng), count(ng);
+        for (int g = 0; g < ng; ++g) { first[g] = ctx->groups[g].traj_first; count[g] = ctx->groups[g].p.ne; }
+        CKA(cudaMemcpy(ctx->d_group_first, first.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
+        CKA(cudaMemcpy(ctx->d_group_count, count.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
+    }
+    if (path == BEC_PATH_FP64_PLAIN) {
+        for (auto &gr : ctx->groups) {
+            CKA(dalloc(ctx, &gr.a, (size_t)gr.p.ne * gr.d.cells));
+            CKA(dalloc(ctx, &gr.b, (size_t)gr.p.ne * gr.d.cells));
+        }
+        CKA(dalloc(ctx, &ctx->scratch_a, (size_t)ctx->max_cells));
+        CKA(dalloc(ctx, &ctx->scratch_b, (size_t)ctx->max_cells));
+        CKA(dalloc(ctx, &ctx->d_plain_obs, (size_t)ctx->n_traj * ctx->max_nz * 4));
+        CKA(dalloc(ctx, &ctx->d_plain_axial, (size_t)ctx->n_traj * ctx->max_nz * 4));
+    } else {
+        std::vector<GroupParamsF> gfs(ng);
+        for (int g = 0; g < ng; ++g) gfs[g] = ctx->groups[g].gf;
+        CKA(dalloc(ctx, &ctx->d_gparams, (size_t)ng));
+        CKA(cudaMemcpy(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice));
+        for (auto &c : ctx->classes) {
+            const size_t nt = (size_t)c.geom.n_traj;
+            c.tiles = fp32_zpass_tiles(c.geom);
+            CKA(dalloc(ctx, &c.state, nt * c.geom.cells));
+            CKA(cudaMemset(c.state, 0, sizeof(float4) * nt * c.geom.cells));
+            CKA(dalloc(ctx, &c.d_tgroup, nt));
+            CKA(dalloc(ctx, &c.d_tlocal, nt));
+            CKA(dalloc(ctx, &c.d_traj_scale, nt));
+            CKA(dalloc(ctx, &c.obs_partial, nt * c.tiles * c.geom.nz * 4));
+            CKA(dalloc(ctx, &c.traj_axial, nt * c.geom.nz * 4));
+            std::vector<int> tg(nt), tl(nt);
+            std::vector<double> ts(nt);
+            for (int g : c.groups) {
+                const GroupRec &gr = ctx->groups[g];
+                for (int t = 0; t < gr.p.ne; ++t) {
+                    tg[gr.local_first + t] = g;
+                    tl[gr.local_first + t] = t;
+                    ts[gr.local_first + t] = (double)c.geom.nx * c.geom.ny * gr.d.dV;
+                }
+            }
+            CKA(cudaMemcpy(c.d_tgroup, tg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
+            CKA(cudaMemcpy(c.d_tlocal, tl.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
+            CKA(cudaMemcpy(c.d_traj_scale, ts.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
+        }
+        CKA(dalloc(ctx, &ctx->scratch4, (size_t)ctx->max_cells));
+    }
+#undef CKA
+    (void)st;
+    *out = ctx;
+    return BEC_OK;
+}
+
+void bec_destroy(bec_ctx *ctx)
+{
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void *p : ctx->allocs) cudaFree(p);
+    for (auto &gr : ctx->groups)
+        if (gr.gs_dev) { /* owned through allocs */ }
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *bec_last_error(const bec_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+bec_status bec_group_info(const bec_ctx *ctx, int32_t group, bec_derived *out)
+{
+    if (!ctx || !out || group < 0 || group >= (int)ctx->groups.size()) return BEC_ERR_INVALID_ARG;
+    *out = ctx->groups[group].d;
+    return BEC_OK;
+}
+
+int64_t bec_total_trajectories(const bec_ctx *ctx) { return ctx ? ctx->n_traj : 0; }
+
+// ------------------------------------------------------------------------ ground state
+bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts, double *psi_out,
+                            bec_gs_report *rep)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!opts || !psi_out || group < 0 || group >= (int)ctx->groups.size())
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad ground-state arguments");
+    if (opts->mode < BEC_GS_FIXED_STEPS || opts->mode > BEC_GS_REFERENCE_E)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "unknown ground-state mode");
+    GroupRec &gr = ctx->groups[group];
+    const GeomD &g = gr.gd;
+    const int cells = g.cells;
+    cudaStream_t s = ctx->stream;
+    const long long l0 = g_launches;
+    double2 *a = nullptr, *tmp = nullptr, *tmp2 = nullptr;
+    {
+        void *pa = nullptr, *pt = nullptr, *pt2 = nullptr;
+        CKC(cudaMalloc(&pa, sizeof(double2) * cells));
+        if (cudaMalloc(&pt, sizeof(double2) * cells) != cudaSuccess ||
+            cudaMalloc(&pt2, sizeof(double2) * cells) != cudaSuccess) {
+            cudaFree(pa); cudaFree(pt);
+            return fail(ctx, BEC_ERR_OUT_OF_MEMORY, "ground-state buffers");
+        }
+        a = (double2 *)pa; tmp = (double2 *)pt; tmp2 = (double2 *)pt2;
+    }
+    struct Guard { void *p[3]; ~Guard() { for (void *q : p) cudaFree(q); } } guard{{a, tmp, tmp2}};
+    double *sc = ctx->d_scal;
+    double *red = ctx->d_red;
+    bec_status st;
+
+    CKC(cudaEventRecord(ctx->ev0, s));
+    if (opts->warm_start) {
+        CKC(cudaMemcpyAsync(a, opts->warm_start, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+    } else {
+        plain_gs_tf(a, g, gr.d.mu, s);                                  // wigner.cu:97
+    }
+    plain_norm(a, cells, sc, red, s);                                   // :101-103
+    plain_renorm(a, cells, sc, gr.d.N, g.dV, s);
+    if ((st = plain_fft(ctx, a, g, 1))) return st;                      // :106-107
+    plain_scale(a, cells, 1.0 / cells, s);
+    CKL();
+
+    const int maxs = opts->max_steps > 0 ? opts->max_steps : 1;
+    const int check = opts->check_every > 0 ? opts->check_every : 1;
+    double E = 0.0, mu_prev = 0.0;
+    int steps = 0, converged = 0;
+    auto measure_mu = [&](double *mu_out) -> bec_status {
+        // x-space sums of the renormalised state, then the Parseval kinetic sum
+        plain_gs_xsums(a, g, sc + 8, red, s);
+        CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
+        bec_status st2 = plain_fft(ctx, tmp, g, 1);
+        if (st2) return st2;
+        plain_scale(tmp, cells, 1.0 / cells, s);
+        plain_gs_ksum(tmp, g, sc + 12, red, s);
+        double h[8];
+        CKC(cudaMemcpyAsync(h, sc + 8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+        CKC(cudaStreamSynchronize(s));
+        const double ekin = h[4] * cells * g.dV, epot = h[0] * g.dV, eint = g.g11 * h[1] * g.dV, N = h[2] * g.dV;
+        *mu_out = (ekin + epot + eint) / N;
+        return BEC_OK;
+    };
+    while (steps < maxs) {
+        plain_gs_kick(a, g, s);                                         // :117
+        if ((st = plain_fft(ctx, a, g, 0))) return st;                  // :121
+        plain_gs_nl(a, g, s);                                           // :124
+        if ((st = plain_fft(ctx, a, g, 1))) return st;                  // :129-130
+        plain_scale(a, cells, 1.0 / cells, s);
+        plain_gs_kick(a, g, s);                                         // :134
+        if ((st = plain_fft(ctx, a, g, 0))) return st;                  // :140
+        plain_norm(a, cells, sc, red, s);                               // :143-145
+        plain_renorm(a, cells, sc, gr.d.N, g.dV, s);
+        CKL();
+        ++steps;
+        bool stop = false;
+        if (opts->mode == BEC_GS_REFERENCE_E) {
+            CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
+            if ((st = plain_fft(ctx, tmp, g, 1))) return st;
+            plain_scale(tmp, cells, 1.0 / cells, s);
+            plain_gs_ref_energy(a, tmp, g, sc + 1, red, s);
+            double hE;
+            CKC(cudaMemcpyAsync(&hE, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+            CKC(cudaStreamSynchronize(s));
+            const double newE = hE * g.dV;
+            if (std::fabs((newE - E) / newE) < 0.000001) stop = true;   // :155
+            E = newE;
+        } else if (opts->mode == BEC_GS_MU && (steps % check) == 0) {
+            double mu;
+            if ((st = measure_mu(&mu))) return st;
+            if (!std::isfinite(mu)) return fail(ctx, BEC_ERR_NUMERICAL, "ground state diverged");
+            if (mu_prev != 0.0 && std::fabs((mu - mu_prev) / mu) < opts->tol) stop = true;
+            mu_prev = mu;
+        }
+        if ((st = plain_fft(ctx, a, g, 1))) return st;                  // :151-152
+        plain_scale(a, cells, 1.0 / cells, s);
+        if (stop) { converged = 1; break; }
+    }
+    if ((st = plain_fft(ctx, a, g, 0))) return st;                      // :163
+    CKC(cudaEventRecord(ctx->ev1, s));
+    CKC(cudaMemcpyAsync(psi_out, a, sizeof(double2) * cells, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (rep) {
+        std::memset(rep, 0, sizeof(*rep));
+        rep->steps = steps;
+        rep->converged = converged;
+        rep->seconds = ms * 1e-3;
+        // mu, energy, residual of the final state
+        plain_gs_xsums(a, g, sc + 8, red, s);
+        CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
+        if ((st = plain_fft(ctx, tmp, g, 1))) return st;
+        plain_scale(tmp, cells, 1.0 / cells, s);
+        plain_gs_ksum(tmp, g, sc + 12, red, s);
+        double h[8];
+        CKC(cudaMemcpyAsync(h, sc + 8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+        CKC(cudaStreamSynchronize(s));
+        const double ekin = h[4] * cells * g.dV, epot = h[0] * g.dV, eint = g.g11 * h[1] * g.dV, N = h[2] * g.dV;
+        const double mu = (ekin + epot + eint) / N;
+        rep->mu = mu;
+        rep->energy = (ekin + epot + 0.5 * eint) / N;
+        rep->N = N;
+        plain_mul_k2(tmp, tmp2, g, s);
+        if ((st = plain_fft(ctx, tmp2, g, 0))) return st;
+        plain_gs_residual(a, tmp2, g, mu, sc + 16, red, s);
+        double r2;
+        CKC(cudaMemcpyAsync(&r2, sc + 16, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CKC(cudaStreamSynchronize(s));
+        rep->residual = std::sqrt(r2 / h[2]);
+    }
+    CKL();
+    ctx->last_launches = g_launches - l0;
+    return BEC_OK;
+}
+
+bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
+                                  double *const *psi_out, bec_gs_report *reports)
+{
+    if (!ctx || n < 0 || (n > 0 && (!groups || !psi_out))) return BEC_ERR_INVALID_ARG;
+    for (int i = 0; i < n; ++i) {
+        bec_status st = bec_ground_state(ctx, groups[i], opts, psi_out[i], reports ? &reports[i] : nullptr);
+        if (st) return st;
+    }
+    return BEC_OK;
+}
+
+// ------------------------------------------------------------------------ evolution
+bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!psi_gs || group < 0 || group >= (int)ctx->groups.size())
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad init arguments");
+    GroupRec &gr = ctx->groups[group];
+    const GeomD &g = gr.gd;
+    const int cells = g.cells, ne = gr.p.ne;
+    cudaStream_t s = ctx->stream;
+    bec_status st;
+    const long long l0 = g_launches;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        double2 *gs = ctx->scratch_a, *nz = nullptr;
+        CKC(cudaMemcpyAsync(gs, psi_gs, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        if (noise) {
+            void *p = nullptr;
+            CKC(cudaMalloc(&p, sizeof(double2) * 2 * (size_t)cells * ne));
+            nz = (double2 *)p;
+            cudaError_t e = cudaMemcpyAsync(nz, noise, sizeof(double2) * 2 * (size_t)cells * ne,
+                                            cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) { cudaFree(p); return fail(ctx, BEC_ERR_CUDA, cudaGetErrorString(e)); }
+        }
+        for (int t = 0; t < ne; ++t) {
+            double2 *a = gr.a + (size_t)t * cells, *b = gr.b + (size_t)t * cells;
+            plain_init(a, b, gs, nz ? nz + (size_t)(2 * t) * cells : nullptr,
+                       nz ? nz + (size_t)(2 * t + 1) * cells : nullptr, g, (uint32_t)t, s);
+            if ((st = plain_fft(ctx, a, g, 1))) { if (nz) { cudaStreamSynchronize(s); cudaFree(nz); } return st; }
+            if ((st = plain_fft(ctx, b, g, 1))) { if (nz) { cudaStreamSynchronize(s); cudaFree(nz); } return st; }
+            plain_scale(a, cells, 1.0 / cells, s);
+            plain_scale(b, cells, 1.0 / cells, s);
+        }
+        if (nz) { cudaStreamSynchronize(s); cudaFree(nz); }
+        CKL();
+    } else {
+        // bring the other groups to a clean step boundary first
+        if ((st = batched_resolve(ctx, false))) return st;
+        if (!gr.gs_dev) CKC(dalloc(ctx, &gr.gs_dev, (size_t)cells));
+        CKC(cudaMemcpyAsync(gr.gs_dev, psi_gs, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        float2 *nz = nullptr;
+        if (noise) {
+            std::vector<float2> h((size_t)2 * cells * ne);
+            for (size_t i = 0; i < h.size(); ++i) h[i] = make_float2((float)noise[2 * i], (float)noise[2 * i + 1]);
+            void *p = nullptr;
+            CKC(cudaMalloc(&p, sizeof(float2) * h.size()));
+            nz = (float2 *)p;
+            cudaError_t e = cudaMemcpy(nz, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { cudaFree(p); return fail(ctx, BEC_ERR_CUDA, cudaGetErrorString(e)); }
+        }
+        ClassRec &c = ctx->classes[gr.cls];
+        float4 *base = c.state + (size_t)gr.local_first * cells;
+        fp32_init_group(base, cells, ne, gr.gf, gr.gs_dev, nz, s);
+        ClassGeom sub = c.geom;
+        sub.n_traj = ne;
+        float2 *tx, *ty;
+        if ((st = get_tw32(ctx, sub.nx, &tx)) || (st = get_tw32(ctx, sub.ny, &ty))) {
+            if (nz) { cudaStreamSynchronize(s); cudaFree(nz); }
+            return st;
+        }
+        fp32_prep(base, sub, tx, ty, s);
+        if (nz) { cudaStreamSynchronize(s); cudaFree(nz); }
+        CKL();
+    }
+    gr.initialised = true;
+    ctx->last_launches = g_launches - l0;
+    return BEC_OK;
+}
+
+bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (n_steps < 0) return fail(ctx, BEC_ERR_INVALID_ARG, "negative step count");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    const long long l0 = g_launches;
+    CKC(cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((st = do_evolve(ctx, n_steps))) return st;
+    CKC(cudaEventRecord(ctx->ev1, ctx->stream));
+    CKC(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = g_launches - l0;
+    return BEC_OK;
+}
+
+bec_status bec_pulse(bec_ctx *ctx, double theta, double phi)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    double2 m[4];
+    rotation(theta, phi, m);
+    return apply_pulse(ctx, m);
+}
+
+bec_status bec_start_evolution(bec_ctx *ctx)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    int neq = ctx->groups[0].d.n_equil_steps;
+    for (auto &g : ctx->groups)
+        if (g.d.n_equil_steps != neq)
+            return fail(ctx, BEC_ERR_INVALID_ARG, "groups disagree on the equilibration step count");
+    if ((st = do_evolve(ctx, neq))) return st;                     // wigner.cu:222-223
+    double2 m[4];
+    rotation(M_PI / 2.0, 0.0, m);                                   // wigner.cu:225
+    if ((st = apply_pulse(ctx, m))) return st;
+    ctx->evo_steps = 0;
+    CKC(cudaStreamSynchronize(ctx->stream));
+    return BEC_OK;
+}
+
+bec_status bec_moments_now(bec_ctx *ctx, bec_moments *out)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, BEC_ERR_INVALID_ARG, "null output");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    if ((st = observe_now(ctx))) return st;
+    return fetch_group_moments(ctx, out);
+}
+
+bec_status bec_traj_moments_now(bec_ctx *ctx, bec_moments *out)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, BEC_ERR_INVALID_ARG, "null output");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    if ((st = observe_now(ctx))) return st;
+    std::vector<double> h((size_t)ctx->n_traj * 4);
+    CKC(cudaMemcpyAsync(h.data(), ctx->d_traj_tot, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CKC(cudaStreamSynchronize(ctx->stream));
+    for (auto &gr : ctx->groups)
+        for (int t = 0; t < gr.p.ne; ++t) {
+            const int i = gr.traj_first + t;
+            out[i].t = ctx->evo_steps * gr.p.dt_evo;
+            out[i].na = h[i * 4 + 0]; out[i].nb = h[i * 4 + 1];
+            out[i].s_re = h[i * 4 + 2]; out[i].s_im = h[i * 4 + 3];
+        }
+    return BEC_OK;
+}
+
+static bec_status group_axial_host(bec_ctx *ctx, int group, double *out)
+{
+    GroupRec &gr = ctx->groups[group];
+    const int nz = gr.d.nvz;
+    std::vector<double> h;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        h.resize((size_t)gr.p.ne * ctx->max_nz * 4);
+        CKC(cudaMemcpyAsync(h.data(), ctx->d_plain_axial + (size_t)gr.traj_first * ctx->max_nz * 4,
+                            sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+        ClassRec &c = ctx->classes[gr.cls];
+        h.resize((size_t)gr.p.ne * nz * 4);
+        CKC(cudaMemcpyAsync(h.data(), c.traj_axial + (size_t)gr.local_first * nz * 4, sizeof(double) * h.size(),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CKC(cudaStreamSynchronize(ctx->stream));
+    const int row = (ctx->path == BEC_PATH_FP64_PLAIN) ? ctx->max_nz : nz;
+    for (int z = 0; z < nz; ++z)
+        for (int k = 0; k < 4; ++k) {
+            HSum acc;
+            for (int t = 0; t < gr.p.ne; ++t) acc.add(h[((size_t)t * row + z) * 4 + k]);
+            out[4 * z + k] = acc.value();
+        }
+    return BEC_OK;
+}
+
+bec_status bec_axial_now(bec_ctx *ctx, int32_t group, double *out)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!out || group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, BEC_ERR_INVALID_ARG, "bad axial args");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    if ((st = observe_now(ctx))) return st;
+    return group_axial_host(ctx, group, out);
+}
+
+bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, double *axial)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!sch || !samples || sch->n_steps < 0 || sch->sample_every < 0 || (sch->axial && !axial))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad schedule");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    const int n = sch->n_steps;
+    const int every = sch->sample_every > 0 ? sch->sample_every : (n > 0 ? n : 1);
+    const int n_samples = n / every;
+    const size_t ng = ctx->groups.size();
+    size_t axial_stride = 0;
+    for (auto &g : ctx->groups) axial_stride += (size_t)4 * g.d.nvz;
+    double2 pi_m[4];
+    rotation(M_PI, 0.0, pi_m);
+    const long long l0 = g_launches;
+    CKC(cudaEventRecord(ctx->ev0, ctx->stream));
+    int sample = 0;
+    auto take_sample = [&]() -> bec_status {
+        bec_status st2 = fetch_group_moments(ctx, samples + (size_t)sample * ng);
+        if (st2) return st2;
+        if (sch->axial) {
+            double *dst = axial + (size_t)sample * axial_stride;
+            for (size_t g = 0; g < ng; ++g) {
+                if ((st2 = group_axial_host(ctx, (int)g, dst))) return st2;
+                dst += 4 * ctx->groups[g].d.nvz;
+            }
+        }
+        ++sample;
+        return BEC_OK;
+    };
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        for (int i = 1; i <= n; ++i) {
+            if ((st = do_evolve(ctx, 1))) return st;
+            if (i % every == 0 && sample < n_samples) {
+                if ((st = plain_observe(ctx))) return st;
+                if ((st = take_sample())) return st;
+            }
+            if (i == sch->pi_pulse_step && (st = apply_pulse(ctx, pi_m))) return st;
+        }
+    } else {
+        bool obs_due = false;
+        for (int i = 1; i <= n; ++i) {
+            // z pass: finishes step i-1 (observing its end state if due), starts step i
+            const double2 *m2 = nullptr;
+            if (i - 1 == sch->pi_pulse_step) m2 = pi_m;
+            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, obs_due, m2))) return st;
+            ctx->pending = true;
+            if (obs_due) {
+                if ((st = batched_reduce_obs(ctx))) return st;
+                // moments belong to the boundary before this step
+                ctx->evo_steps--;
+                st = take_sample();
+                ctx->evo_steps++;
+                if (st) return st;
+                obs_due = false;
+            }
+            if ((st = batched_ppass_all(ctx))) return st;
+            ctx->step++;
+            ctx->evo_steps++;
+            if (i % every == 0 && sample < n_samples) obs_due = true;
+        }
+        if (obs_due) {
+            if ((st = batched_resolve(ctx, true))) return st;
+            if ((st = batched_reduce_obs(ctx))) return st;
+            if ((st = take_sample())) return st;
+        }
+        if (n == sch->pi_pulse_step && (st = apply_pulse(ctx, pi_m))) return st;
+    }
+    CKC(cudaEventRecord(ctx->ev1, ctx->stream));
+    CKC(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = g_launches - l0;
+    return BEC_OK;
+}
+
+bec_status bec_observables(const bec_ctx *ctx, int32_t group, const bec_moments *m, bec_obs *out)
+{
+    if (!ctx || !m || !out || group < 0 || group >= (int)ctx->groups.size()) return BEC_ERR_INVALID_ARG;
+    const GroupRec &gr = ctx->groups[group];
+    const double ne = gr.p.ne;
+    // Wigner term: density subtracts V/(2 dV) per cell (wigner_kernel.cu:283-286), i.e. V/2 per cell after * dV
+    const double sub = ne * gr.d.cells * gr.d.V / 2.0;
+    const double N1 = m->na - sub, N2 = m->nb - sub;
+    out->t = m->t;
+    out->N1 = N1 / ne;
+    out->N2 = N2 / ne;
+    out->Ntotal = (N1 + N2) / ne;
+    const double S = std::hypot(m->s_re, m->s_im);
+    out->visibility = 2.0 * S / (N1 + N2);
+    out->phase = std::atan2(m->s_im, m->s_re);
+    double mx = 0.0;
+    for (double alpha = 0; alpha < 2 * M_PI; alpha += 0.5) {      // wigner.cu:270
+        const double im = std::sin(alpha) * m->s_re + std::cos(alpha) * m->s_im;   // Im(e^{i alpha} S)
+        const double n1 = std::fabs((m->na + m->nb) / 2.0 + im - sub);
+        const double n2 = std::fabs((m->na + m->nb) / 2.0 - im - sub);
+        const double r = (n1 - n2) / (n1 + n2);
+        if (std::fabs(r) > mx) mx = std::fabs(r);
+    }
+    out->visibility_scan = mx;
+    return BEC_OK;
+}
+
+bec_status bec_phase_scan(const bec_ctx *ctx, int32_t group, const bec_moments *m, int32_t n_alpha,
+                          const double *alpha, double *out)
+{
+    if (!ctx || !m || n_alpha < 0 || (n_alpha > 0 && (!alpha || !out)) || group < 0 ||
+        group >= (int)ctx->groups.size())
+        return BEC_ERR_INVALID_ARG;
+    const GroupRec &gr = ctx->groups[group];
+    const double ne = gr.p.ne;
+    const double sub = ne * gr.d.cells * gr.d.V / 2.0;
+    for (int j = 0; j < n_alpha; ++j) {
+        const double im = std::sin(alpha[j]) * m->s_re + std::cos(alpha[j]) * m->s_im;
+        out[2 * j] = ((m->na + m->nb) / 2.0 + im - sub) / ne;
+        out[2 * j + 1] = ((m->na + m->nb) / 2.0 - im - sub) / ne;
+    }
+    return BEC_OK;
+}
+
+// ------------------------------------------------------------------------ state I/O
+bec_status bec_get_state(bec_ctx *ctx, int32_t group, int32_t traj, double *ab)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!ab || group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, BEC_ERR_INVALID_ARG, "bad args");
+    GroupRec &gr = ctx->groups[group];
+    if (traj < 0 || traj >= gr.p.ne) return fail(ctx, BEC_ERR_INVALID_ARG, "bad trajectory");
+    if (!gr.initialised) return fail(ctx, BEC_ERR_STATE, "group not initialised");
+    const int cells = gr.d.cells;
+    cudaStream_t s = ctx->stream;
+    bec_status st;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        CKC(cudaMemcpyAsync(ctx->scratch_a, gr.a + (size_t)traj * cells, sizeof(double2) * cells,
+                            cudaMemcpyDeviceToDevice, s));
+        CKC(cudaMemcpyAsync(ctx->scratch_b, gr.b + (size_t)traj * cells, sizeof(double2) * cells,
+                            cudaMemcpyDeviceToDevice, s));
+        if ((st = plain_fft(ctx, ctx->scratch_a, gr.gd, 0))) return st;
+        if ((st = plain_fft(ctx, ctx->scratch_b, gr.gd, 0))) return st;
+        CKC(cudaMemcpyAsync(ab, ctx->scratch_a, sizeof(double2) * cells, cudaMemcpyDeviceToHost, s));
+        CKC(cudaMemcpyAsync(ab + 2 * (size_t)cells, ctx->scratch_b, sizeof(double2) * cells, cudaMemcpyDeviceToHost, s));
+        CKC(cudaStreamSynchronize(s));
+        return BEC_OK;
+    }
+    if ((st = batched_resolve(ctx, false))) return st;
+    ClassRec &c = ctx->classes[gr.cls];
+    CKC(cudaMemcpyAsync(ctx->scratch4, c.state + (size_t)(gr.local_first + traj) * cells, sizeof(float4) * cells,
+                        cudaMemcpyDeviceToDevice, s));
+    ClassGeom one = c.geom;
+    one.n_traj = 1;
+    float2 *tx, *ty;
+    if ((st = get_tw32(ctx, one.nx, &tx)) || (st = get_tw32(ctx, one.ny, &ty))) return st;
+    fp32_unprep(ctx->scratch4, one, tx, ty, s);
+    // the stored representation carries the unnormalised x-y inverse transform
+    std::vector<float4> h(cells);
+    CKC(cudaMemcpyAsync(h.data(), ctx->scratch4, sizeof(float4) * cells, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    const double inv = 1.0 / ((double)one.nx * one.ny);
+    for (int i = 0; i < cells; ++i) {
+        ab[2 * i] = h[i].x * inv; ab[2 * i + 1] = h[i].y * inv;
+        ab[2 * ((size_t)cells + i)] = h[i].z * inv; ab[2 * ((size_t)cells + i) + 1] = h[i].w * inv;
+    }
+    return BEC_OK;
+}
+
+bec_status bec_set_state(bec_ctx *ctx, int32_t group, int32_t traj, const double *ab)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!ab || group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, BEC_ERR_INVALID_ARG, "bad args");
+    GroupRec &gr = ctx->groups[group];
+    if (traj < 0 || traj >= gr.p.ne) return fail(ctx, BEC_ERR_INVALID_ARG, "bad trajectory");
+    const int cells = gr.d.cells;
+    cudaStream_t s = ctx->stream;
+    bec_status st;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        double2 *a = gr.a + (size_t)traj * cells, *b = gr.b + (size_t)traj * cells;
+        CKC(cudaMemcpyAsync(a, ab, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        CKC(cudaMemcpyAsync(b, ab + 2 * (size_t)cells, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        if ((st = plain_fft(ctx, a, gr.gd, 1))) return st;
+        if ((st = plain_fft(ctx, b, gr.gd, 1))) return st;
+        plain_scale(a, cells, 1.0 / cells, s);
+        plain_scale(b, cells, 1.0 / cells, s);
+        CKC(cudaStreamSynchronize(s));
+        CKL();
+        gr.initialised = true;
+        return BEC_OK;
+    }
+    if ((st = batched_resolve(ctx, false))) return st;
+    std::vector<float4> h(cells);
+    for (int i = 0; i < cells; ++i)
+        h[i] = make_float4((float)ab[2 * i], (float)ab[2 * i + 1], (float)ab[2 * ((size_t)cells + i)],
+                           (float)ab[2 * ((size_t)cells + i) + 1]);
+    ClassRec &c = ctx->classes[gr.cls];
+    float4 *dst = c.state + (size_t)(gr.local_first + traj) * cells;
+    CKC(cudaMemcpyAsync(dst, h.data(), sizeof(float4) * cells, cudaMemcpyHostToDevice, s));
+    ClassGeom one = c.geom;
+    one.n_traj = 1;
+    float2 *tx, *ty;
+    if ((st = get_tw32(ctx, one.nx, &tx)) || (st = get_tw32(ctx, one.ny, &ty))) return st;
+    fp32_prep(dst, one, tx, ty, s);
+    CKC(cudaStreamSynchronize(s));
+    CKL();
+    gr.initialised = true;
+    return BEC_OK;
+}
+
+int64_t bec_step_index(const bec_ctx *ctx) { return ctx ? ctx->step : -1; }
+double bec_last_device_ms(const bec_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+int64_t bec_last_launch_count(const bec_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+} // extern "C"

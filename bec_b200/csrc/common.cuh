@@ -1,0 +1,134 @@
+// common.cuh -- device helpers shared by the FP64 plain and FP32 batched paths:
+// complex arithmetic on float2/double2 (and float4 = a pair of complex values
+// for the two components of one cell), Philox4x32-10 and Box-Muller.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define BEC_HD __host__ __device__ __forceinline__
+
+// ---------------------------------------------------------------- complex
+BEC_HD double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+BEC_HD float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+BEC_HD double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+BEC_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+BEC_HD double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+BEC_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+BEC_HD double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+BEC_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+BEC_HD double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+BEC_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// float4 holds (a.re, a.im, b.re, b.im): both components of one cell.
+BEC_HD float4 pmul(float4 v, float2 w)
+{
+    return make_float4(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x,
+                       v.z * w.x - v.w * w.y, v.z * w.y + v.w * w.x);
+}
+BEC_HD float4 padd(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+BEC_HD float4 psub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+BEC_HD float4 pscale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+
+// Twiddle multiply used by the FFT stages, overloaded on the element type.
+BEC_HD double2 tmul(double2 v, double2 w) { return cmul(v, w); }
+BEC_HD float2 tmul(float2 v, float2 w) { return cmul(v, w); }
+BEC_HD float4 tmul(float4 v, float2 w) { return pmul(v, w); }
+BEC_HD double2 vadd(double2 a, double2 b) { return cadd(a, b); }
+BEC_HD float2 vadd(float2 a, float2 b) { return cadd(a, b); }
+BEC_HD float4 vadd(float4 a, float4 b) { return padd(a, b); }
+BEC_HD double2 vsub(double2 a, double2 b) { return csub(a, b); }
+BEC_HD float2 vsub(float2 a, float2 b) { return csub(a, b); }
+BEC_HD float4 vsub(float4 a, float4 b) { return psub(a, b); }
+
+// ---------------------------------------------------------------- Philox4x32-10
+// Counter-based generator of Salmon, Moraes, Dror and Shaw (SC'11):
+// ten rounds of two 32x32->64 multiplies with Weyl-sequence key bumps.
+struct u32x4 { uint32_t x, y, z, w; };
+
+BEC_HD u32x4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+        uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return u32x4{c0, c1, c2, c3};
+}
+
+// Stream tags of the counter's fourth word.
+enum { RNG_TAG_INIT = 0, RNG_TAG_LOSS1 = 1, RNG_TAG_LOSS2 = 2 };
+
+// Box-Muller from two 32-bit words. u1 = (x1 + 1) / 2^32 in (0, 1],
+// u2 = x2 / 2^32; -ln(u1) is taken through log1p near u1 = 1 so both tails
+// keep full relative precision.
+__device__ __forceinline__ void box_muller(uint32_t x1, uint32_t x2, double &n1, double &n2)
+{
+    double nl = (x1 < 0x80000000u) ? -log(((double)x1 + 1.0) * 0x1p-32)
+                                   : -log1p(-((double)(0xFFFFFFFFu - x1)) * 0x1p-32);
+    double r = sqrt(2.0 * nl);
+    double s, c;
+    sincospi(2.0 * ((double)x2 * 0x1p-32), &s, &c);
+    n1 = r * c;
+    n2 = r * s;
+}
+
+__device__ __forceinline__ void box_muller(uint32_t x1, uint32_t x2, float &n1, float &n2)
+{
+    float nl = (x1 < 0x80000000u) ? -logf(((float)x1 + 1.0f) * 0x1p-32f)
+                                  : -log1pf(-((float)(0xFFFFFFFFu - x1)) * 0x1p-32f);
+    float r = sqrtf(2.0f * nl);
+    float s, c;
+    sincospif(2.0f * ((float)x2 * 0x1p-32f), &s, &c);
+    n1 = r * c;
+    n2 = r * s;
+}
+
+// Four standard normals for (seed, trajectory, step, cell, tag).
+template <typename R>
+__device__ __forceinline__ void normals4(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell,
+                                         uint32_t tag, R out[4])
+{
+    u32x4 r = philox4x32_10(cell, step, traj, tag, (uint32_t)seed, (uint32_t)(seed >> 32));
+    box_muller(r.x, r.y, out[0], out[1]);
+    box_muller(r.z, r.w, out[2], out[3]);
+}
+
+// ---------------------------------------------------------------- misc
+__host__ __device__ __forceinline__ int brev_bits(int v, int bits)
+{
+#ifdef __CUDA_ARCH__
+    return bits ? (int)(__brev((unsigned)v) >> (32 - bits)) : 0;
+#else
+    int r = 0;
+    for (int b = 0; b < bits; ++b) if (v & (1 << b)) r |= 1 << (bits - 1 - b);
+    return r;
+#endif
+}
+
+// k value of lattice index i (getK, wigner_kernel.cu:15-21)
+template <typename R>
+__host__ __device__ __forceinline__ R getk(int i, R dk, int n) { return (2 * i > n) ? dk * (R)(i - n) : dk * (R)i; }
+
+// Neumaier-compensated accumulator.
+struct KSum {
+    double s, c;
+    __host__ __device__ KSum() : s(0.0), c(0.0) {}
+    __host__ __device__ void add(double v)
+    {
+        double t = s + v;
+        if (fabs(s) >= fabs(v)) c += (s - t) + v; else c += (v - t) + s;
+        s = t;
+    }
+    __host__ __device__ double value() const { return s + c; }
+};

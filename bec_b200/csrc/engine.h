@@ -1,0 +1,113 @@
+// engine.h -- internal interfaces between the C-ABI host code (bec_api.cpp)
+// and the kernel files (plain_fp64.cu, batched_fp32.cu, reduce.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/bec.h"
+
+// ----------------------------------------------------------------------------
+// FP64 per-group geometry and physics, passed by value to the plain kernels.
+struct GeomD {
+    int nx, ny, nz, lx, ly, lz, cells;
+    double dkx, dky, dkz;
+    double xmax, ymax, zmax, dx, dy, dz, lambda;
+    double g11, g12, g22, l111, l12, l22, detuning;
+    double dt_evo, dt_steady, dV;
+    double Va, Vb;
+    int itmax, noise;
+    uint64_t seed;
+};
+
+// FP32 per-group parameters of the batched path (device array, one per group).
+struct GroupParamsF {
+    float dkx, dky, dkz;
+    float xmax, ymax, zmax, dx, dy, dz, inv_lambda2;
+    float g11, g12, g22, l111, l12, l22, detuning;
+    float dt;                 // dt_evo, natural units
+    float noise_amp;          // sqrt(dt / (2 dV))
+    float c1, c2, c3;         // loss-noise amplitudes 3 sqrt(l111/6), sqrt(l12/2), sqrt(l22)
+    float init_a, init_b;     // Va / sqrt(dV), Vb / sqrt(dV)
+    int itmax, noise;
+    uint32_t seed_lo, seed_hi;
+};
+
+// Geometry of one grid class of the batched path (all trajectories sharing nx, ny, nz).
+struct ClassGeom {
+    int nx, ny, nz, lx, ly, lz, cells;
+    int n_traj;
+};
+
+// ----------------------------------------------------------------------------
+// plain_fp64.cu (one trajectory at a time; a, b point at that trajectory)
+void plain_kick(double2 *a, double2 *b, const GeomD &g, double scale, int apply_scale, cudaStream_t s);
+void plain_fft3d(double2 *data, const GeomD &g, const double2 *tw_x, const double2 *tw_y,
+                 const double2 *tw_z, int inv, cudaStream_t s);
+void plain_nl(double2 *a, double2 *b, const GeomD &g, uint32_t traj, uint32_t step, cudaStream_t s);
+void plain_scale(double2 *a, int n, double scale, cudaStream_t s);
+void plain_pulse(double2 *a, double2 *b, int n, double2 m11, double2 m12, double2 m21, double2 m22,
+                 cudaStream_t s);
+void plain_init(double2 *a, double2 *b, const double2 *gs, const double2 *noise_a, const double2 *noise_b,
+                const GeomD &g, uint32_t traj, cudaStream_t s);
+// per-z sums (|a|^2, |b|^2, Re, Im conj(a) b) of x-space arrays into out[nz][4], accumulating
+void plain_axial_sums(const double2 *a, const double2 *b, const GeomD &g, double *out, cudaStream_t s);
+// ground state
+void plain_gs_tf(double2 *a, const GeomD &g, double mu, cudaStream_t s);
+void plain_gs_kick(double2 *a, const GeomD &g, cudaStream_t s);
+void plain_gs_nl(double2 *a, const GeomD &g, cudaStream_t s);
+// sums of |a|^2 into out[0] (device scalar, Neumaier); tmp has >= 2*1024 doubles
+void plain_norm(const double2 *a, int n, double *out, double *tmp, cudaStream_t s);
+// a *= sqrt(N / (sum * dV)) with sum read from device memory
+void plain_renorm(double2 *a, int n, const double *sum, double N, double dV, cudaStream_t s);
+// x-space sums: out[0] = sum n V, out[1] = sum n^2, out[2] = sum n
+void plain_gs_xsums(const double2 *a, const GeomD &g, double *out, double *tmp, cudaStream_t s);
+// k-space sum of |ak|^2 k^2/2 into out[0]
+void plain_gs_ksum(const double2 *ak, const GeomD &g, double *out, double *tmp, cudaStream_t s);
+// reference energy integrand sum (wigner_kernel.cu:232-258) into out[0]
+void plain_gs_ref_energy(const double2 *ax, const double2 *ak, const GeomD &g, double *out, double *tmp,
+                         cudaStream_t s);
+// h = (V + g11 n - mu) psi + hk (hk = FORWARD(psik k^2/2)); out[0] = sum |h|^2
+void plain_gs_residual(const double2 *ax, const double2 *hk, const GeomD &g, double mu, double *out,
+                       double *tmp, cudaStream_t s);
+// hk = ak * k^2/2
+void plain_mul_k2(const double2 *ak, double2 *hk, const GeomD &g, cudaStream_t s);
+
+// ----------------------------------------------------------------------------
+// batched_fp32.cu
+struct ZPassArgs {
+    float pre;            // kick fraction before the observation (0 or 0.5)
+    float post;           // kick fraction after it (0 or 0.5)
+    float scale;          // applied after the inverse z transform (1 / cells)
+    float out_scale;      // applied before the forward z transform: 1 when a plane pass
+                          // follows, nx*ny when the pass ends a step (see batched_fp32.cu)
+    int has_m1;           // 1: apply matrix m1 before the observation
+    float2 m1[4];         // row-major 2x2 (m11, m12, m21, m22)
+    int observe;          // 1: write per-z partial moments
+    int has_m2;           // 1: apply matrix m2 after the observation
+    float2 m2[4];
+};
+
+// x-space initial state of ne consecutive trajectories of one group (GS + vacuum noise);
+// noise == NULL draws from Philox, else [traj][a|b][cell] float2
+void fp32_init_group(float4 *state, int cells, int ne, const GroupParamsF &gp, const double2 *gs,
+                     const float2 *noise, cudaStream_t s);
+// x-space -> stored representation (inverse transform over x and y)
+void fp32_prep(float4 *state, const ClassGeom &c, const float2 *tw_x, const float2 *tw_y, cudaStream_t s);
+// stored representation -> x-space (forward transform over x and y)
+void fp32_unprep(float4 *state, const ClassGeom &c, const float2 *tw_x, const float2 *tw_y, cudaStream_t s);
+void fp32_zpass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
+                const float2 *tw_z, const ZPassArgs &z, double *obs_partial, cudaStream_t s);
+void fp32_ppass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
+                const int *tlocal, const float2 *tw_x, const float2 *tw_y, uint32_t step, cudaStream_t s);
+int fp32_zpass_tiles(const ClassGeom &c);   // tiles per trajectory of the z pass (obs_partial layout)
+// obs_partial[traj][tile][z][4] -> traj_axial[traj][z][4] * traj_scale[traj] (1 if NULL),
+// traj_tot[traj][4] = sum over z; traj_axial may be NULL
+void obs_reduce(const double *obs_partial, int n_traj, int tiles, int nz, const double *traj_scale,
+                double *traj_axial, double *traj_tot, cudaStream_t s);
+// group sums: for g: out[g][4] = sum_{t in group} traj_tot[t]; trajectories of a group are contiguous
+void group_reduce(const double *traj_tot, const int *group_first, const int *group_count, int n_groups,
+                  double *out, cudaStream_t s);
+
+// launch counter (kernels this library enqueued since the counter was reset)
+extern thread_local long long g_launches;

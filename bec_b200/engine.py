@@ -1,0 +1,253 @@
+"""ctypes binding of libbec.so (include/bec.h).
+
+This is the Python face of the engine: `Engine` owns a bec_ctx and mirrors the
+reference's host entry points (programs/bec_wigner_3d.cuda/wigner.cpp:32-40):
+calculateSteadyState -> ground_state, initEvolution -> init_group +
+start_evolution, calculateEvolution -> evolve / run, plus observables.
+
+There is no CPU fallback: if the CUDA library cannot be loaded or no device
+is visible, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (BecDerived, BecGsOpts, BecGsReport, BecMoments, BecObs, BecParams, BecSchedule,
+                   BEC_GS_FIXED_STEPS, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbec.so")
+
+_lib = None
+
+# every function of include/bec.h: name -> (restype, argtypes)
+_P = C.POINTER
+_dp = _P(C.c_double)
+SIGNATURES = {
+    "bec_abi_version": (C.c_int32, []),
+    "bec_derive_params": (C.c_int, [_P(BecParams), _P(BecDerived)]),
+    "bec_create": (C.c_int, [_P(BecParams), C.c_int32, C.c_int32, _P(C.c_void_p)]),
+    "bec_destroy": (None, [C.c_void_p]),
+    "bec_last_error": (C.c_char_p, [C.c_void_p]),
+    "bec_group_info": (C.c_int, [C.c_void_p, C.c_int32, _P(BecDerived)]),
+    "bec_total_trajectories": (C.c_int64, [C.c_void_p]),
+    "bec_ground_state": (C.c_int, [C.c_void_p, C.c_int32, _P(BecGsOpts), _dp, _P(BecGsReport)]),
+    "bec_ground_state_batch": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32), _P(BecGsOpts), _P(_dp),
+                                         _P(BecGsReport)]),
+    "bec_init_group": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
+    "bec_evolve": (C.c_int, [C.c_void_p, C.c_int32]),
+    "bec_pulse": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "bec_start_evolution": (C.c_int, [C.c_void_p]),
+    "bec_moments_now": (C.c_int, [C.c_void_p, _P(BecMoments)]),
+    "bec_axial_now": (C.c_int, [C.c_void_p, C.c_int32, _dp]),
+    "bec_traj_moments_now": (C.c_int, [C.c_void_p, _P(BecMoments)]),
+    "bec_run": (C.c_int, [C.c_void_p, _P(BecSchedule), _P(BecMoments), _dp]),
+    "bec_observables": (C.c_int, [C.c_void_p, C.c_int32, _P(BecMoments), _P(BecObs)]),
+    "bec_phase_scan": (C.c_int, [C.c_void_p, C.c_int32, _P(BecMoments), C.c_int32, _dp, _dp]),
+    "bec_get_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
+    "bec_set_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
+    "bec_step_index": (C.c_int64, [C.c_void_p]),
+    "bec_last_device_ms": (C.c_double, [C.c_void_p]),
+    "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
+}
+
+
+class BecError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Loads libbec.so (building it first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build
+            build.build()
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def derive(p):
+    d = BecDerived()
+    st = lib().bec_derive_params(C.byref(p), C.byref(d))
+    if st:
+        raise BecError(st, "bec_derive_params")
+    return d
+
+
+class Engine:
+    """A bec_ctx: one or more ensembles ("groups") on the current CUDA device."""
+
+    def __init__(self, groups, path=BEC_PATH_FP32_BATCHED):
+        if isinstance(groups, BecParams):
+            groups = [groups]
+        self.params = list(groups)
+        arr = (BecParams * len(self.params))(*self.params)
+        h = C.c_void_p()
+        st = lib().bec_create(arr, len(self.params), path, C.byref(h))
+        if st:
+            raise BecError(st, "bec_create")
+        self._h = h
+        self.path = path
+        self.derived = [self._info(g) for g in range(len(self.params))]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bec_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st:
+            raise BecError(st, f"{what}: {lib().bec_last_error(self._h).decode()}")
+
+    def _info(self, g):
+        d = BecDerived()
+        self._check(lib().bec_group_info(self._h, g, C.byref(d)), "bec_group_info")
+        return d
+
+    @property
+    def n_groups(self):
+        return len(self.params)
+
+    @property
+    def n_traj(self):
+        return int(lib().bec_total_trajectories(self._h))
+
+    @property
+    def step_index(self):
+        return int(lib().bec_step_index(self._h))
+
+    @property
+    def last_device_ms(self):
+        return float(lib().bec_last_device_ms(self._h))
+
+    @property
+    def last_launch_count(self):
+        return int(lib().bec_last_launch_count(self._h))
+
+    # ---- ground state (calculateSteadyState, wigner.cu:84-175)
+    def ground_state(self, group=0, mode=BEC_GS_FIXED_STEPS, max_steps=100, tol=1e-6, check_every=1,
+                     warm_start=None):
+        d = self.derived[group]
+        o = BecGsOpts()
+        o.mode, o.max_steps, o.check_every, o.tol = mode, max_steps, check_every, tol
+        ws = None
+        if warm_start is not None:
+            ws = np.ascontiguousarray(warm_start, dtype=np.complex128).reshape(-1)
+            if ws.size != d.cells:
+                raise ValueError("warm start size")
+            o.warm_start = _dptr(ws.view(np.float64))
+        psi = np.zeros(d.cells, dtype=np.complex128)
+        rep = BecGsReport()
+        self._check(lib().bec_ground_state(self._h, group, C.byref(o), _dptr(psi.view(np.float64)),
+                                           C.byref(rep)), "bec_ground_state")
+        return psi, rep
+
+    # ---- ensembles (initEvolution, wigner.cu:202-227)
+    def init_group(self, group, psi_gs, noise=None):
+        d = self.derived[group]
+        g = np.ascontiguousarray(psi_gs, dtype=np.complex128).reshape(-1)
+        if g.size != d.cells:
+            raise ValueError("ground-state size")
+        nz = None
+        if noise is not None:
+            nz = np.ascontiguousarray(noise, dtype=np.complex128).reshape(-1)
+            if nz.size != 2 * d.cells * self.params[group].ne:
+                raise ValueError("noise size")
+        self._check(lib().bec_init_group(self._h, group, _dptr(g.view(np.float64)),
+                                         _dptr(nz.view(np.float64)) if nz is not None else None),
+                    "bec_init_group")
+
+    def start_evolution(self):
+        self._check(lib().bec_start_evolution(self._h), "bec_start_evolution")
+
+    def evolve(self, n):
+        self._check(lib().bec_evolve(self._h, int(n)), "bec_evolve")
+
+    def pulse(self, theta, phi=0.0):
+        self._check(lib().bec_pulse(self._h, float(theta), float(phi)), "bec_pulse")
+
+    # ---- observables
+    def moments(self):
+        ms = (BecMoments * self.n_groups)()
+        self._check(lib().bec_moments_now(self._h, ms), "bec_moments_now")
+        return np.array([[m.t, m.na, m.nb, m.s_re, m.s_im] for m in ms])
+
+    def traj_moments(self):
+        ms = (BecMoments * self.n_traj)()
+        self._check(lib().bec_traj_moments_now(self._h, ms), "bec_traj_moments_now")
+        return np.array([[m.t, m.na, m.nb, m.s_re, m.s_im] for m in ms])
+
+    def axial(self, group=0):
+        out = np.zeros((self.derived[group].nvz, 4))
+        self._check(lib().bec_axial_now(self._h, group, _dptr(out)), "bec_axial_now")
+        return out
+
+    def observables(self, group, moments_row):
+        m = BecMoments(*[float(v) for v in moments_row])
+        o = BecObs()
+        self._check(lib().bec_observables(self._h, group, C.byref(m), C.byref(o)), "bec_observables")
+        return {k: getattr(o, k) for k, _ in BecObs._fields_}
+
+    def phase_scan(self, group, moments_row, alphas):
+        m = BecMoments(*[float(v) for v in moments_row])
+        al = np.ascontiguousarray(alphas, dtype=np.float64)
+        out = np.zeros(2 * al.size)
+        self._check(lib().bec_phase_scan(self._h, group, C.byref(m), al.size, _dptr(al), _dptr(out)),
+                    "bec_phase_scan")
+        return out.reshape(-1, 2)
+
+    def run(self, n_steps, sample_every=0, pi_pulse_step=-1, axial=False):
+        """Runs n_steps, returning moments [n_samples, n_groups, 5] (and axial profiles)."""
+        s = BecSchedule(int(n_steps), int(sample_every), int(pi_pulse_step), int(bool(axial)))
+        every = sample_every if sample_every > 0 else max(n_steps, 1)
+        n_samples = n_steps // every
+        ms = (BecMoments * max(n_samples * self.n_groups, 1))()
+        ax = None
+        if axial:
+            ax = np.zeros(max(n_samples, 1) * sum(4 * d.nvz for d in self.derived))
+        self._check(lib().bec_run(self._h, C.byref(s), ms, _dptr(ax) if ax is not None else None), "bec_run")
+        mom = np.array([[m.t, m.na, m.nb, m.s_re, m.s_im] for m in ms][: n_samples * self.n_groups])
+        mom = mom.reshape(n_samples, self.n_groups, 5)
+        if axial:
+            out, off = [], 0
+            for d in self.derived:
+                out.append(ax.reshape(max(n_samples, 1), -1)[:n_samples, off:off + 4 * d.nvz].reshape(n_samples, d.nvz, 4))
+                off += 4 * d.nvz
+            return mom, out
+        return mom
+
+    # ---- state I/O (checkpoint / parity)
+    def get_state(self, group, traj):
+        d = self.derived[group]
+        ab = np.zeros(2 * d.cells, dtype=np.complex128)
+        self._check(lib().bec_get_state(self._h, group, traj, _dptr(ab.view(np.float64))), "bec_get_state")
+        return ab.reshape(2, d.cells)
+
+    def set_state(self, group, traj, ab):
+        ab = np.ascontiguousarray(ab, dtype=np.complex128).reshape(-1)
+        self._check(lib().bec_set_state(self._h, group, traj, _dptr(ab.view(np.float64))), "bec_set_state")
+
+
+__all__ = ["Engine", "BecError", "derive", "lib", "BEC_PATH_FP32_BATCHED", "BEC_PATH_FP64_PLAIN"]

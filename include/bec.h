@@ -1,0 +1,270 @@
+/*
+ * bec.h -- C ABI of the B200 split-step Gross-Pitaevskii / truncated-Wigner engine.
+ *
+ * Plain C types only: pointers, sizes, doubles. No CUDA or C++ types cross this
+ * boundary, so any FFI (ctypes, cgo, JNI, N-API) can bind it.
+ *
+ * The reference reaches its hot path through free C functions declared in
+ * programs/bec_wigner_3d.cuda/wigner.cpp:32-40 (initConstants,
+ * calculateSteadyState, initEvolution, calculateEvolution, initWaveVectors,
+ * releaseWaveVectors) that read a process-global __constant__ parameter block
+ * and texture (wigner_kernel.cu:8-12) and abort the process on any error
+ * (cutilSafeCall). This ABI keeps the same operations and parameter surface
+ * (defines.h:25-54) but
+ *   - holds all state in an explicit context (one per host thread),
+ *   - returns a status code instead of aborting,
+ *   - lets the caller own every host array and the context own device memory.
+ *
+ * Complex arrays on the host are interleaved doubles (re, im), x fastest:
+ * index = ((z * nvy + y) * nvx + x)  (wigner_kernel.cu:29-34, :101-106).
+ */
+#ifndef BEC_H
+#define BEC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEC_ABI_VERSION 1
+
+typedef enum bec_status {
+    BEC_OK = 0,
+    BEC_ERR_INVALID_ARG = 1,      /* bad pointer, size or parameter value */
+    BEC_ERR_UNSUPPORTED_GRID = 2, /* grid not a supported power-of-two shape */
+    BEC_ERR_CUDA = 3,             /* a CUDA runtime call failed; see bec_last_error */
+    BEC_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed */
+    BEC_ERR_STATE = 5,            /* call out of order (e.g. evolve before init) */
+    BEC_ERR_NUMERICAL = 6,        /* NaN/Inf or norm blow-up detected in a reduction */
+    BEC_ERR_NO_DEVICE = 7,        /* no CUDA device visible */
+    BEC_ERR_UNIMPLEMENTED = 8
+} bec_status;
+
+/* Execution paths. */
+enum {
+    /* One trajectory at a time, one kernel per operation, FP64 throughout:
+     * structured like the reference's propagate() (wigner.cu:178-199). */
+    BEC_PATH_FP64_PLAIN = 0,
+    /* All trajectories of all groups in fused FP32 passes with FP64
+     * compensated reductions; the product path. */
+    BEC_PATH_FP32_BATCHED = 1
+};
+
+/*
+ * Model parameters of one ensemble ("group"), real units.
+ * Mirrors ModelParameters (programs/bec_wigner_3d.cuda/defines.h:25-54) with
+ * three differences: the loss rates are SI (m^6/s for gamma111, m^3/s for
+ * gamma12/gamma22; the reference takes cm units and divides by 1e12 / 1e6 in
+ * wigner.cpp:141-143), nvy == 1 selects a 2D x-z slice, and the loss-noise
+ * switch and RNG seed are explicit.
+ */
+typedef struct bec_params {
+    double a11, a12, a22;          /* scattering lengths, Bohr radii */
+    double m;                      /* particle mass, kg */
+    double fx, fy, fz;             /* trap frequencies, Hz (fy only renormalises 2D) */
+    double N;                      /* atom number */
+    double detuning;               /* Hz */
+    double gamma111;               /* three-body loss, m^6/s */
+    double gamma12, gamma22;       /* two-body losses, m^3/s */
+    double Va, Vb;                 /* vacuum-noise weights (0 = none, 1 = full) */
+    int32_t nvx, nvy, nvz;         /* grid points; powers of two; nvy == 1 => 2D */
+    int32_t itmax;                 /* midpoint iterations of the nonlinear step */
+    double dt_steady;              /* imaginary-time step, s */
+    double t_equilib;              /* equilibration time before the first pi/2, s */
+    double dt_evo;                 /* real-time step, s */
+    int32_t ne;                    /* trajectories in this ensemble */
+    int32_t loss_noise;            /* 1: add the Wigner loss-noise terms */
+    uint64_t seed;                 /* Philox key for this ensemble */
+} bec_params;
+
+/*
+ * Derived parameters in natural units (l_rho = sqrt(hbar/(m w_x)), t_rho = 1/w_x).
+ * Mirrors CalculationParameters (defines.h:57-112) as filled by
+ * fillDerivedParameters (wigner.cpp:119-176), in FP64, including the
+ * reference's dk = pi / xmax (wigner.cpp:167-169).
+ */
+typedef struct bec_derived {
+    double N;
+    double g11, g12, g22;          /* couplings (2D: divided by sqrt(2 pi) l_y) */
+    double mu;                     /* Thomas-Fermi chemical potential */
+    double Va, Vb, V;              /* V = (Va + Vb) / 2 */
+    double lambda;                 /* fx / fz */
+    double l_rho, t_rho;           /* natural length (m) and time (s) */
+    double detuning;               /* natural units */
+    double l111, l12, l22;         /* loss rates, natural units */
+    double xmax, ymax, zmax;       /* box half-widths */
+    double dx, dy, dz;             /* space steps (dy = 1 in 2D) */
+    double dkx, dky, dkz;          /* k steps */
+    double dV;                     /* cell volume dx*dy*dz (dx*dz in 2D) */
+    double dt_steady, t_equilib, dt_evo;
+    int32_t nvx, nvy, nvz;
+    int32_t cells;
+    int32_t itmax;
+    int32_t ne;
+    int32_t dims;                  /* 2 or 3 */
+    int32_t n_equil_steps;         /* steps taken by the equilibration loop (wigner.cu:222) */
+} bec_derived;
+
+/* Ground-state stopping rules. */
+enum {
+    BEC_GS_FIXED_STEPS = 0,  /* exactly max_steps imaginary-time steps */
+    BEC_GS_MU = 1,           /* stop when |d mu| / mu < tol between checks */
+    BEC_GS_REFERENCE_E = 2   /* the reference's |dE/E| < 1e-6 test on its energy integral (wigner.cu:148-156) */
+};
+
+typedef struct bec_gs_opts {
+    int32_t mode;            /* BEC_GS_* */
+    int32_t max_steps;       /* step cap (the exact count for FIXED_STEPS) */
+    int32_t check_every;     /* steps between convergence checks (MU mode) */
+    int32_t reserved;
+    double tol;              /* relative tolerance for MU mode (REFERENCE_E uses 1e-6) */
+    const double *warm_start;/* optional x-space start (interleaved complex, cells); NULL = Thomas-Fermi */
+} bec_gs_opts;
+
+typedef struct bec_gs_report {
+    int32_t steps;           /* imaginary-time steps taken */
+    int32_t converged;       /* 1 if the stopping rule was met before max_steps */
+    double mu;               /* chemical potential (Parseval kinetic + potential + 2x interaction) / N */
+    double energy;           /* energy per particle */
+    double N;                /* norm after the last renormalisation */
+    double residual;         /* || H psi - mu psi || / || psi || */
+    double seconds;          /* device time of the loop */
+} bec_gs_report;
+
+/*
+ * Per-sample FP64 moments of one ensemble, summed over its trajectories
+ * (compensated summation on the device):
+ *   na = sum |a|^2 dV,  nb = sum |b|^2 dV,  s = sum conj(a) b dV.
+ * All of the reference's observables are closed-form functions of these:
+ * see bec_observables().
+ */
+typedef struct bec_moments {
+    double t;                /* physical time since the first pi/2 pulse, s */
+    double na, nb;
+    double s_re, s_im;
+} bec_moments;
+
+/* Observables derived from moments (no device work). */
+typedef struct bec_obs {
+    double t;
+    double N1, N2;           /* per-trajectory populations, Wigner term V/(2 dV) subtracted (wigner_kernel.cu:283-286) */
+    double Ntotal;           /* the reference's printed population after its second pi/2 (wigner.cu:363-369) */
+    double visibility;       /* 2 |<psi1|psi2>| / (N1 + N2)  (report.tex:855-860) */
+    double visibility_scan;  /* max over alpha = 0, 0.5, ... < 2 pi of |N1-N2|/(N1+N2) (wigner.cu:267-277) */
+    double phase;            /* arg <psi1|psi2>, reference sign convention */
+} bec_obs;
+
+/* Run schedule for bec_run. Time zero is the state at call time. */
+typedef struct bec_schedule {
+    int32_t n_steps;         /* real-time steps to take */
+    int32_t sample_every;    /* record moments after every k-th step (0: only after the last) */
+    int32_t pi_pulse_step;   /* apply a pi pulse after this step count (-1: none) */
+    int32_t axial;           /* 1: also record axial (z) projections per sample */
+} bec_schedule;
+
+typedef struct bec_ctx bec_ctx;
+
+/* ---- parameters ------------------------------------------------------- */
+
+/* fillDerivedParameters (wigner.cpp:119-176), FP64, SI loss rates. */
+bec_status bec_derive_params(const bec_params *p, bec_derived *out);
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Creates a context holding n_groups ensembles on the current CUDA device.
+ * Replaces initConstants + initWaveVectors + EvolutionState::init
+ * (wigner_kernel.cu:395-399, :25-55; defines.h:157-184). */
+bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, bec_ctx **out);
+void bec_destroy(bec_ctx *ctx);                         /* releaseWaveVectors + EvolutionState::release */
+const char *bec_last_error(const bec_ctx *ctx);         /* message of the last failing call ("" if none) */
+int32_t bec_abi_version(void);
+bec_status bec_group_info(const bec_ctx *ctx, int32_t group, bec_derived *out);
+int64_t bec_total_trajectories(const bec_ctx *ctx);
+
+/* ---- ground state ----------------------------------------------------- */
+
+/* calculateSteadyState (wigner.cu:84-175) for one group's parameters:
+ * imaginary-time split-step from Thomas-Fermi (or a warm start), renormalised
+ * to N after every step. psi_out receives the x-space ground state
+ * (interleaved complex, cells). */
+bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts,
+                            double *psi_out, bec_gs_report *report);
+
+/* Ground states for several groups at once (batched), one stopping rule. */
+bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups,
+                                  const bec_gs_opts *opts, double *const *psi_out,
+                                  bec_gs_report *reports);
+
+/* ---- evolution -------------------------------------------------------- */
+
+/* initializeEnsembles (wigner_kernel.cu:295-317) for one group:
+ *   a = psi_gs + Va * eta_a / sqrt(dV),  b = Vb * eta_b / sqrt(dV),
+ * eta complex normal with <|eta|^2> = 1/2. noise == NULL draws eta from
+ * Philox4x32-10 keyed by (seed, trajectory); otherwise noise holds
+ * ne * 2 * cells interleaved complex values laid out [traj][a|b][cell]. */
+bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise);
+
+/* Advances every trajectory by n real-time split steps (propagate, wigner.cu:178-199). */
+bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps);
+
+/* Instantaneous Rabi rotation of every trajectory (report.tex rotation matrix):
+ *   a' = cos(theta/2) a - i e^{-i phi} sin(theta/2) b
+ *   b' = -i e^{i phi} sin(theta/2) a + cos(theta/2) b.
+ * theta = pi/2, phi = 0 is applyHalfPiPulse (wigner_kernel.cu:320-329);
+ * theta = pi, phi = 0 is applyPiPulse (:332-341). */
+bec_status bec_pulse(bec_ctx *ctx, double theta, double phi);
+
+/* The reference's initEvolution (wigner.cu:202-227) after bec_init_group for every
+ * group: the equilibration steps (t = 0; t <= t_equilib; t += dt_evo), then the
+ * first pi/2 pulse. Resets the time origin to zero. */
+bec_status bec_start_evolution(bec_ctx *ctx);
+
+/* Moments of every group at the current time; out has n_groups entries. */
+bec_status bec_moments_now(bec_ctx *ctx, bec_moments *out);
+
+/* Axial profiles of one group at the current time: for each z,
+ * out[4*z + 0..3] = (sum_xy |a|^2 dV, sum_xy |b|^2 dV, Re, Im of sum_xy conj(a) b dV),
+ * summed over the group's trajectories. out has 4 * nvz doubles. */
+bec_status bec_axial_now(bec_ctx *ctx, int32_t group, double *out);
+
+/* Per-trajectory moments at the current time: n_traj entries, trajectories
+ * ordered by group then index. */
+bec_status bec_traj_moments_now(bec_ctx *ctx, bec_moments *out);
+
+/* Runs a schedule. samples receives n_samples * n_groups moments
+ * (sample-major), n_samples = n_steps / sample_every (or 1). When
+ * schedule->axial is set, axial receives n_samples * sum_g(4 * nvz_g) doubles
+ * (sample-major, groups in order); otherwise it may be NULL. */
+bec_status bec_run(bec_ctx *ctx, const bec_schedule *schedule, bec_moments *samples, double *axial);
+
+/* Observables of one group from its moments (pure host arithmetic). */
+bec_status bec_observables(const bec_ctx *ctx, int32_t group, const bec_moments *m, bec_obs *out);
+
+/* Rotated populations after a final pi/2 pulse about axis angle alpha (halfPiRotate,
+ * wigner_kernel.cu:344-360) for n_alpha angles: out[2*j], out[2*j+1] = N1(alpha_j), N2(alpha_j),
+ * per trajectory, Wigner term subtracted. */
+bec_status bec_phase_scan(const bec_ctx *ctx, int32_t group, const bec_moments *m,
+                          int32_t n_alpha, const double *alpha, double *out);
+
+/* ---- state I/O (checkpoint / parity) ---------------------------------- */
+
+/* x-space state of one trajectory of one group: a then b, each cells
+ * interleaved complex (2 * cells complex values). */
+bec_status bec_get_state(bec_ctx *ctx, int32_t group, int32_t traj, double *ab_out);
+bec_status bec_set_state(bec_ctx *ctx, int32_t group, int32_t traj, const double *ab_in);
+int64_t bec_step_index(const bec_ctx *ctx);
+
+/* ---- timing ----------------------------------------------------------- */
+
+/* Device time of the last bec_evolve / bec_run call, milliseconds (CUDA events). */
+double bec_last_device_ms(const bec_ctx *ctx);
+/* Number of this library's kernel launches issued by the last bec_evolve / bec_run. */
+int64_t bec_last_launch_count(const bec_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEC_H */

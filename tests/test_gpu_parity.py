@@ -1,0 +1,228 @@
+"""Parity of the CUDA engine (called through the C ABI) against the CPU FP64 oracle.
+
+Tolerances:
+  FP64 plain path ........ 1e-10 relative (states and moments), the bar of the
+                           reference's own CPU path restated in FP64.
+  FP32 batched path ...... per-trajectory states within FP32_STATE_* of the
+                           oracle's max |psi|; moments within FP32_MOM relative;
+                           visibility within 1e-4 absolute.
+"""
+import numpy as np
+import pytest
+
+from bec_b200 import observables as OBS
+from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_REFERENCE_E
+from bec_b200.configs import config0, config1, copy_params, rb87_params
+from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
+from oracle import oracle as O
+from parity_util import engine_sequence, moments_rel_err, oracle_sequence, record, rel_state_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_STATE_SHORT = 2e-4     # <= 200 steps
+FP32_STATE_LONG = 3e-3      # 2500 steps
+FP32_MOM = 1e-4
+FP32_VIS = 1e-4
+
+PATHS = [BEC_PATH_FP64_PLAIN, BEC_PATH_FP32_BATCHED]
+
+
+@pytest.fixture(scope="module")
+def cfg0_gs():
+    p = config0()
+    psi, rep = O.ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=2000)
+    return p, psi
+
+
+# ------------------------------------------------------------------ ground state
+def test_fp64_ground_state_config0_2000_steps(cfg0_gs):
+    """2D 32x128, 2000 imaginary-time steps from Thomas-Fermi."""
+    p, psi_o = cfg0_gs
+    eng = Engine([p], path=BEC_PATH_FP64_PLAIN)
+    psi, rep = eng.ground_state(0, mode=BEC_GS_FIXED_STEPS, max_steps=2000)
+    err = rel_state_err(psi, psi_o)
+    record("gs_config0_fp64", state_err=err)
+    assert rep.steps == 2000
+    assert err < FP64_TOL
+    mu_o, e_o, r_o, n_o = O.gs_measures(p, psi_o)
+    assert rep.mu == pytest.approx(mu_o, rel=1e-10)
+    assert rep.energy == pytest.approx(e_o, rel=1e-10)
+    assert rep.N == pytest.approx(n_o, rel=1e-12)
+    assert rep.residual == pytest.approx(r_o, rel=1e-6)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_ground_state_modes_3d(path):
+    p = rb87_params(N=30000, grid=(16, 16, 128))
+    eng = Engine([p], path=path)
+    psi, rep = eng.ground_state(0, mode=BEC_GS_MU, max_steps=3000, tol=1e-7, check_every=10)
+    psi_o, rep_o = O.ground_state(p, mode=BEC_GS_MU, max_steps=3000, tol=1e-7, check_every=10)
+    assert rep.converged and rep.steps == rep_o.steps
+    assert rel_state_err(psi, psi_o) < 1e-9
+    assert rep.mu == pytest.approx(rep_o.mu, rel=1e-10)
+    psi2, rep2 = eng.ground_state(0, mode=BEC_GS_REFERENCE_E, max_steps=20000)
+    psi2_o, rep2_o = O.ground_state(p, mode=BEC_GS_REFERENCE_E, max_steps=20000)
+    assert rep2.steps == rep2_o.steps
+    assert rel_state_err(psi2, psi2_o) < 1e-9
+
+
+def test_ground_state_warm_start():
+    p = rb87_params(N=30000, grid=(8, 8, 64))
+    eng = Engine([p], path=BEC_PATH_FP32_BATCHED)
+    psi, _ = eng.ground_state(0, max_steps=300)
+    psi_o, _ = O.ground_state(p, max_steps=300)
+    assert rel_state_err(psi, psi_o) < 1e-10
+    _, cold = eng.ground_state(0, mode=BEC_GS_MU, max_steps=5000, tol=1e-6, check_every=5)
+    _, warm = eng.ground_state(0, mode=BEC_GS_MU, max_steps=5000, tol=1e-6, check_every=5, warm_start=psi)
+    assert cold.converged and warm.converged
+    assert warm.steps < cold.steps
+
+
+# ------------------------------------------------------------------ configs[0] evolution
+@pytest.mark.parametrize("path", PATHS)
+def test_config0_evolution(cfg0_gs, path):
+    """pi/2 then 100 ms (2500 steps), no noise, samples every 250 steps."""
+    p, gs = cfg0_gs
+    mo, eo = oracle_sequence(p, gs, 2500, 250)
+    me, ee = engine_sequence(p, gs, 2500, 250, path)
+    assert me.shape == mo.shape
+    np.testing.assert_allclose(me[:, 0], mo[:, 0], rtol=1e-12)
+    tol_m = FP64_TOL if path == BEC_PATH_FP64_PLAIN else FP32_MOM
+    worst_m = max(max(moments_rel_err(a, b)) for a, b in zip(me, mo))
+    d = eo.d
+    vis_e = [OBS.visibility(m, d, 1) for m in me]
+    vis_o = [OBS.visibility(m, d, 1) for m in mo]
+    vis_err = float(np.max(np.abs(np.array(vis_e) - np.array(vis_o))))
+    st_err = rel_state_err(ee.get_state(0, 0), eo.get_state(0))
+    record(f"config0_path{path}", moments_err=worst_m, vis_err=vis_err, state_err=st_err)
+    assert worst_m < tol_m
+    assert st_err < (FP64_TOL if path == BEC_PATH_FP64_PLAIN else FP32_STATE_LONG)
+    assert vis_err < (1e-10 if path == BEC_PATH_FP64_PLAIN else FP32_VIS)
+
+
+# ------------------------------------------------------------------ Wigner noise, per trajectory
+@pytest.mark.parametrize("path", PATHS)
+def test_wigner_noise_per_trajectory(path):
+    """Philox initial noise + loss noise, 16x16x128, 3 trajectories, 150 steps: the same
+    counter-based draws on both sides, so each trajectory matches."""
+    p = rb87_params(N=30000, grid=(16, 16, 128), ne=3, noise=True, seed=11)
+    gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=300)
+    mo, eo = oracle_sequence(p, gs, 150, 50)
+    me, ee = engine_sequence(p, gs, 150, 50, path)
+    tol_s = 1e-9 if path == BEC_PATH_FP64_PLAIN else FP32_STATE_SHORT
+    worst = 0.0
+    for t in range(p.ne):
+        worst = max(worst, rel_state_err(ee.get_state(0, t), eo.get_state(t)))
+    tm_e, tm_o = ee.traj_moments(), eo.traj_moments()
+    tm_err = float(np.max(np.abs(tm_e[:, 1:3] - tm_o[:, 1:3]) / tm_o[:, 1:3]))
+    record(f"noise_traj_path{path}", state_err=worst, traj_mom_err=tm_err)
+    assert worst < tol_s
+    assert tm_err < (1e-10 if path == BEC_PATH_FP64_PLAIN else FP32_MOM)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_injected_noise_arrays(path):
+    """Trajectories driven by caller-supplied initial noise arrays."""
+    p = rb87_params(N=20000, grid=(8, 8, 64), ne=2, noise=True, loss_noise=False)
+    d = O.derive(p)
+    rng = np.random.default_rng(5)
+    noise = 0.5 * (rng.standard_normal((2, 2, d.cells)) + 1j * rng.standard_normal((2, 2, d.cells)))
+    gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=200)
+    mo, eo = oracle_sequence(p, gs, 100, 100, noise=noise)
+    me, ee = engine_sequence(p, gs, 100, 100, path, noise=noise)
+    tol_s = 1e-10 if path == BEC_PATH_FP64_PLAIN else FP32_STATE_SHORT
+    for t in range(p.ne):
+        assert rel_state_err(ee.get_state(0, t), eo.get_state(t)) < tol_s
+
+
+# ------------------------------------------------------------------ uneven batch
+def test_uneven_batch_fp32():
+    """Mixed grids and atom numbers in one context (one launch per pass and grid class)."""
+    groups = [
+        rb87_params(N=15000, grid=(8, 8, 64), ne=2, noise=True, seed=1, fx=92.0, fy=92.0),
+        rb87_params(N=40000, grid=(16, 16, 128), ne=1, noise=True, seed=2, fz=12.5),
+        rb87_params(N=25000, grid=(32, 1, 128), ne=2, noise=True, seed=3),
+        rb87_params(N=60000, grid=(8, 8, 64), ne=1, noise=False, seed=4),
+    ]
+    eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
+    gss, ens = [], []
+    for g, p in enumerate(groups):
+        gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=200)
+        gss.append(gs)
+        eng.init_group(g, gs)
+        e = O.OracleEnsemble(p)
+        e.init(gs)
+        e.start_evolution()
+        ens.append(e)
+    eng.start_evolution()
+    mom = eng.run(60, sample_every=30)
+    for e in ens:
+        e.evolve(60)
+    for g, (p, e) in enumerate(zip(groups, ens)):
+        mo = e.moments()
+        err = moments_rel_err(mom[-1, g], mo)
+        assert max(err) < FP32_MOM, (g, err)
+        for t in range(p.ne):
+            assert rel_state_err(eng.get_state(g, t), e.get_state(t)) < FP32_STATE_SHORT
+
+
+# ------------------------------------------------------------------ schedule, pulses, observables
+@pytest.mark.parametrize("path", PATHS)
+def test_run_with_pi_pulse_and_axial(path):
+    """Spin echo: pi pulse after 40 of 80 steps; samples every 20 with axial profiles."""
+    p = rb87_params(N=30000, grid=(8, 8, 64), ne=2, noise=True, seed=9)
+    gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=200)
+    mo, eo = oracle_sequence(p, gs, 80, 20, pi_pulse_step=40)
+    eng = Engine([p], path=path)
+    eng.init_group(0, gs)
+    eng.start_evolution()
+    mom, axial = eng.run(80, sample_every=20, pi_pulse_step=40, axial=True)
+    tol = 1e-10 if path == BEC_PATH_FP64_PLAIN else FP32_MOM
+    for a, b in zip(mom[:, 0], mo):
+        assert max(moments_rel_err(a, b)) < tol
+    ax_o = eo.axial()
+    ax_e = axial[0][-1]
+    # the last sample precedes nothing else, so it is the oracle's final state
+    np.testing.assert_allclose(ax_e[:, :2], ax_o[:, :2], rtol=tol * 10, atol=tol * ax_o[:, :2].max())
+    np.testing.assert_allclose(OBS.axial_ratio(ax_e, eo.d, p.ne), eo.ref_axial_ratio(),
+                               atol=1e-8 if path == BEC_PATH_FP64_PLAIN else 1e-3)
+    obs = eng.observables(0, mom[-1, 0])
+    assert obs["visibility_scan"] == pytest.approx(eo.ref_visibility(), abs=1e-9 if path == BEC_PATH_FP64_PLAIN else FP32_VIS)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_evolve_and_run_agree(path):
+    p = rb87_params(N=30000, grid=(8, 8, 64), ne=1, noise=True, seed=3)
+    gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=100)
+    m1, e1 = engine_sequence(p, gs, 30, 10, path, use_run=True)
+    m2, e2 = engine_sequence(p, gs, 30, 10, path, use_run=False)
+    np.testing.assert_allclose(m1, m2, rtol=1e-5 if path else 1e-12)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_state_roundtrip(path):
+    p = rb87_params(N=30000, grid=(16, 16, 128), ne=2)
+    d = O.derive(p)
+    rng = np.random.default_rng(0)
+    ab = rng.standard_normal((2, d.cells)) + 1j * rng.standard_normal((2, d.cells))
+    eng = Engine([p], path=path)
+    eng.init_group(0, np.zeros(d.cells))
+    eng.set_state(0, 1, ab)
+    back = eng.get_state(0, 1)
+    assert rel_state_err(back, ab) < (1e-14 if path == BEC_PATH_FP64_PLAIN else 1e-6)
+
+
+def test_paths_agree_on_config1_ensemble_visibility():
+    """configs[1]-shaped run (16x16x128, 4 trajectories, noise), 250 steps: ensemble
+    visibility of the batched FP32 path within 1e-3 of the FP64 oracle."""
+    p = config1()
+    gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=400)
+    mo, eo = oracle_sequence(p, gs, 250, 50)
+    me, ee = engine_sequence(p, gs, 250, 50, BEC_PATH_FP32_BATCHED)
+    d = eo.d
+    err = max(abs(OBS.visibility(a, d, p.ne) - OBS.visibility(b, d, p.ne)) for a, b in zip(me, mo))
+    perr = max(abs(OBS.phase(a) - OBS.phase(b)) for a, b in zip(me, mo))
+    record("config1_vis", vis_err=err, phase_err=perr)
+    assert err < 1e-3
+    assert perr < 1e-3
