@@ -1058,11 +1058,8 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
             ctx->pending = true;
             if (obs_due) {
                 if ((st = batched_reduce_obs(ctx))) return st;
-                // moments belong to the boundary before this step
-                ctx->evo_steps--;
-                st = take_sample();
-                ctx->evo_steps++;
-                if (st) return st;
+                // the moments belong to the boundary before this step: evo_steps = i - 1
+                if ((st = take_sample())) return st;
                 obs_due = false;
             }
             if ((st = batched_ppass_all(ctx))) return st;
@@ -1212,6 +1209,105 @@ bec_status bec_set_state(bec_ctx *ctx, int32_t group, int32_t traj, const double
     CKC(cudaStreamSynchronize(s));
     CKL();
     gr.initialised = true;
+    return BEC_OK;
+}
+
+bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes, int32_t *dims, int64_t *traj,
+                             double *ms, int32_t *n_classes)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (n_steps < 1 || max_classes < 0 || !n_classes || (max_classes > 0 && (!dims || !traj || !ms)))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad profile arguments");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    cudaStream_t s = ctx->stream;
+    const bool plain = ctx->path == BEC_PATH_FP64_PLAIN;
+    const int nc = plain ? (int)ctx->groups.size() : (int)ctx->classes.size();
+    std::vector<cudaEvent_t> ev;
+    auto new_event = [&]() { cudaEvent_t e; cudaEventCreate(&e); ev.push_back(e); return e; };
+    // [step][class][pass] -> (start, stop)
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks((size_t)n_steps * nc * 2, {nullptr, nullptr});
+    for (int i = 0; i < n_steps; ++i) {
+        if (plain) {
+            for (int g = 0; g < nc; ++g) {
+                GroupRec &gr = ctx->groups[g];
+                auto &mk = marks[((size_t)i * nc + g) * 2];
+                mk.first = new_event();
+                mk.second = new_event();
+                CKC(cudaEventRecord(mk.first, s));
+                for (int t = 0; t < gr.p.ne; ++t)
+                    if ((st = plain_step(ctx, gr, t))) return st;
+                CKC(cudaEventRecord(mk.second, s));
+            }
+        } else {
+            ZPassArgs z{};
+            z.pre = ctx->pending ? 0.5f : 0.0f;
+            z.post = 0.5f;
+            z.out_scale = 1.0f;
+            if (ctx->has_pulse) {
+                z.has_m1 = 1;
+                for (int k = 0; k < 4; ++k) z.m1[k] = make_float2((float)ctx->pulse[k].x, (float)ctx->pulse[k].y);
+            }
+            for (int c = 0; c < nc; ++c) {
+                ClassRec &cr = ctx->classes[c];
+                if (cr.geom.n_traj == 0) continue;
+                float2 *tz;
+                if ((st = get_tw32(ctx, cr.geom.nz, &tz))) return st;
+                z.scale = (float)(1.0 / (double)cr.geom.cells);
+                auto &mk = marks[((size_t)i * nc + c) * 2];
+                mk.first = new_event();
+                mk.second = new_event();
+                CKC(cudaEventRecord(mk.first, s));
+                fp32_zpass(cr.state, cr.geom, ctx->d_gparams, cr.d_tgroup, tz, z, cr.obs_partial, s);
+                CKC(cudaEventRecord(mk.second, s));
+            }
+            ctx->has_pulse = false;
+            ctx->pending = true;
+            for (int c = 0; c < nc; ++c) {
+                ClassRec &cr = ctx->classes[c];
+                if (cr.geom.n_traj == 0) continue;
+                float2 *tx, *ty;
+                if ((st = get_tw32(ctx, cr.geom.nx, &tx)) || (st = get_tw32(ctx, cr.geom.ny, &ty))) return st;
+                auto &mk = marks[((size_t)i * nc + c) * 2 + 1];
+                mk.first = new_event();
+                mk.second = new_event();
+                CKC(cudaEventRecord(mk.first, s));
+                fp32_ppass(cr.state, cr.geom, ctx->d_gparams, cr.d_tgroup, cr.d_tlocal, tx, ty, (uint32_t)ctx->step, s);
+                CKC(cudaEventRecord(mk.second, s));
+            }
+        }
+        CKL();
+        ctx->step++;
+        ctx->evo_steps++;
+    }
+    CKC(cudaStreamSynchronize(s));
+    const int nw = std::min(nc, (int)max_classes);
+    for (int c = 0; c < nw; ++c) {
+        double sum[2] = {0.0, 0.0};
+        for (int i = 0; i < n_steps; ++i)
+            for (int k = 0; k < 2; ++k) {
+                auto &mk = marks[((size_t)i * nc + c) * 2 + k];
+                if (!mk.first) continue;
+                float t = 0.f;
+                cudaEventElapsedTime(&t, mk.first, mk.second);
+                sum[k] += t;
+            }
+        if (plain) {
+            const GroupRec &gr = ctx->groups[c];
+            dims[3 * c] = gr.d.nvx; dims[3 * c + 1] = gr.d.nvy; dims[3 * c + 2] = gr.d.nvz;
+            traj[c] = gr.p.ne;
+            ms[2 * c] = sum[0] / n_steps / gr.p.ne;
+            ms[2 * c + 1] = 0.0;
+        } else {
+            const ClassRec &cr = ctx->classes[c];
+            dims[3 * c] = cr.geom.nx; dims[3 * c + 1] = cr.geom.ny; dims[3 * c + 2] = cr.geom.nz;
+            traj[c] = cr.geom.n_traj;
+            ms[2 * c] = sum[0] / n_steps;
+            ms[2 * c + 1] = sum[1] / n_steps;
+        }
+    }
+    *n_classes = nc;
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
     return BEC_OK;
 }
 

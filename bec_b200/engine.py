@@ -50,6 +50,8 @@ SIGNATURES = {
     "bec_step_index": (C.c_int64, [C.c_void_p]),
     "bec_last_device_ms": (C.c_double, [C.c_void_p]),
     "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
+    "bec_profile_steps": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P(C.c_int32), _P(C.c_int64), _dp,
+                                    _P(C.c_int32)]),
 }
 
 
@@ -237,6 +239,17 @@ class Engine:
                 off += 4 * d.nvz
             return mom, out
         return mom
+
+    def profile_steps(self, n_steps, max_classes=16):
+        """Per grid class: dict(dims, traj, z_ms, plane_ms) mean device time per launch."""
+        dims = (C.c_int32 * (3 * max_classes))()
+        traj = (C.c_int64 * max_classes)()
+        ms = (C.c_double * (2 * max_classes))()
+        nc = C.c_int32()
+        self._check(lib().bec_profile_steps(self._h, int(n_steps), max_classes, dims, traj, ms, C.byref(nc)),
+                    "bec_profile_steps")
+        return [dict(dims=tuple(dims[3 * c:3 * c + 3]), traj=int(traj[c]), z_ms=ms[2 * c], plane_ms=ms[2 * c + 1])
+                for c in range(min(nc.value, max_classes))]
 
     # ---- state I/O (checkpoint / parity)
     def get_state(self, group, traj):

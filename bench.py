@@ -1,0 +1,353 @@
+"""Benchmark: Wigner trajectory-steps per second of the batched FP32 path.
+
+Workload (the batched uneven-ensemble configuration): 1024 trajectories per
+GPU in one context, grids drawn uniformly from 8x8x64, 16x16x128 and
+32x32x256, N ~ U[5000, 70000], trap frequencies jittered +-10 %, Rb-87
+two-body and three-body losses with Wigner loss noise, dt = 40 us. A step is
+one split step of every trajectory. Initial states are Thomas-Fermi profiles
+plus Philox vacuum noise (the cost of a step does not depend on the state).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0. Under torchrun every rank runs its own 1024
+trajectories (weak scaling); the timed region is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# ncu: DRAM bytes (read + write) per launch of the dominant kernel, measured on a
+# 64-trajectory 32x32x256 class (profiles/ppass_32x32x256.md), per trajectory.
+NCU_TRAFFIC_PER_TRAJ = None
+
+N_TRAJ = 1024
+WORKLOAD = "uneven-ensembles-1024"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="bec", choices=["bec", "reference"])
+    ap.add_argument("--n-traj", type=int, default=N_TRAJ)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and CPU baseline legs")
+    ap.add_argument("--grids", default=None,
+                    help="restrict the grid mix, e.g. 32x32x256 or 8x8x64,16x16x128 (profiling captures)")
+    return ap.parse_args()
+
+
+def grid_mix(args):
+    from bec_b200.configs import UNEVEN_GRIDS
+    if not args.grids:
+        return UNEVEN_GRIDS
+    return tuple(tuple(int(v) for v in g.split("x")) for g in args.grids.split(","))
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def thomas_fermi(d):
+    import numpy as np
+    x = -d.xmax + d.dx * np.arange(d.nvx)
+    y = (-d.ymax + d.dy * np.arange(d.nvy)) if d.nvy > 1 else np.zeros(1)
+    z = -d.zmax + d.dz * np.arange(d.nvz)
+    V = (x[None, None, :] ** 2 + y[None, :, None] ** 2 + z[:, None, None] ** 2 / d.lambda_ ** 2) / 2
+    return np.sqrt(np.maximum(d.mu - V, 0.0) / d.g11).reshape(-1).astype(np.complex128)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.f:
+            return None
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(groups, seconds, steps_per_rep=1):
+    """Times the oracle (FP64 CPU restatement) on a bounded sample of the workload,
+    one trajectory per thread on all host cores. Returns (traj-steps/s, cores, sample)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    n = max(3, min(len(groups), 2 * cores))
+    sample = groups[:n]
+    ens = []
+    for p in sample:
+        e = O.OracleEnsemble(p)
+        e.init(thomas_fermi(O.derive(p)))
+        ens.append(e)
+
+    def work(e):
+        e.evolve(steps_per_rep, 1)
+
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        t0 = time.perf_counter()
+        list(ex.map(work, ens))
+        t1 = time.perf_counter()
+        reps = max(1, int(seconds / max(t1 - t0, 1e-3)))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            list(ex.map(work, ens))
+        el = time.perf_counter() - t0
+    v = n * steps_per_rep * reps / el
+    grids = {}
+    for p in sample:
+        k = f"{p.nvx}x{p.nvy}x{p.nvz}"
+        grids[k] = grids.get(k, 0) + 1
+    return v, cores, f"{n} trajectories of the workload mix {grids}, {reps * steps_per_rep} steps, {el:.1f} s"
+
+
+def run_reference(args, ws, rank):
+    from bec_b200.configs import config2
+    if rank != 0:
+        return
+    groups = config2(n_traj=args.n_traj, seed=2, grids=grid_mix(args))
+    vals = []
+    sample = ""
+    cores = os.cpu_count() or 1
+    per = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    for _ in range(args.warmup):
+        cpu_baseline(groups, 0.2)
+    for _ in range(args.steps):
+        v, cores, sample = cpu_baseline(groups, per)
+        vals.append(v)
+    v = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": "wigner_traj_steps_per_s", "value": v, "unit": "traj-steps/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_traj": args.n_traj, "grids": "8x8x64/16x16x128/32x32x256",
+                   "implementation": "CPU FP64 restatement of the reference's split step (oracle port)"},
+        "cpu_baseline": {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if ws > 1:
+        os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
+    if args.impl == "reference":
+        if ws > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo")
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+    from bec_b200.configs import config2
+    from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
+
+    torch.cuda.set_device(0 if ws > 1 else 0)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    groups = config2(n_traj=args.n_traj, seed=2 + 7919 * rank, grids=grid_mix(args))
+    eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
+    # pinned host ground states (Thomas-Fermi), reused by the e2e leg
+    host_gs = []
+    for g, d in enumerate(eng.derived):
+        tf = thomas_fermi(d)
+        pin = torch.empty(2 * d.cells, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+        pin[:] = tf
+        host_gs.append(pin)
+    for g in range(eng.n_groups):
+        eng.init_group(g, host_gs[g])
+    eng.start_evolution()
+    cells = np.array([d.cells for d in eng.derived], dtype=np.float64)
+    total_cells = float(cells.sum())
+
+    # warm-up, then K device-timed steps
+    eng.evolve(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        eng.evolve(args.steps)
+        torch.cuda.synchronize()
+    ms = eng.last_device_ms
+    launches = eng.last_launch_count
+    if ws > 1:
+        dist.barrier()
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n_traj_total = args.n_traj * ws
+    value = n_traj_total * args.steps / (ms * 1e-3)
+
+    # per-kernel device times of the same workload (CUDA events on the engine's stream)
+    prof = eng.profile_steps(3)
+    peak, peak_kind = peaks()
+    kernels = []
+    for c in prof:
+        nx, ny, nz = c["dims"]
+        bytes_launch = 32.0 * nx * ny * nz * c["traj"]      # read + write of both complex64 components
+        for kind, t in (("zpass", c["z_ms"]), ("ppass", c["plane_ms"])):
+            kernels.append(dict(kernel=f"{kind}_{nx}x{ny}x{nz}", ms=t, bytes=bytes_launch, traj=c["traj"]))
+    dom = max(kernels, key=lambda k: k["ms"])
+    achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
+    traffic = None
+    if NCU_TRAFFIC_PER_TRAJ and dom["kernel"] in NCU_TRAFFIC_PER_TRAJ:
+        traffic = NCU_TRAFFIC_PER_TRAJ[dom["kernel"]] * dom["traj"]
+    roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "algorithmic_bytes": dom["bytes"], "ms_per_launch": dom["ms"]}
+    step_gbs = 32.0 * total_cells * args.steps / (ms * 1e-3) / 1e9 * (ws if ws > 1 else 1)
+    step_roof = {"achieved": step_gbs / ws if ws > 1 else step_gbs, "peak": peak, "unit": "GB/s",
+                 "frac": (step_gbs / ws if ws > 1 else step_gbs) / peak,
+                 "note": "32 B/cell/step algorithmic bytes of the whole step, all kernels"}
+
+    # e2e through the C ABI: host ground states (pinned) -> init -> pi/2 -> K steps -> moments to host
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for g in range(eng.n_groups):
+        eng.init_group(g, host_gs[g])
+    eng.start_evolution()
+    every = max(1, args.steps // 4)
+    mom = eng.run(args.steps, sample_every=every)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = 16.0 * total_cells / args.steps
+    d2h = 40.0 * mom.shape[0] * mom.shape[1] / args.steps
+    e2e = {"value": n_traj_total * args.steps / e2e_s, "unit": "traj-steps/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "note": "init from pinned host ground states + pi/2 + K steps + moments to host, per call"}
+
+    # ensemble observables: one small FP64 all-reduce of the per-sample moments (weak scaling)
+    if ws > 1:
+        t = torch.tensor(mom[:, :, 1:].sum(axis=1), dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+
+    extras = {}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_extras:
+        # plain per-trajectory FP64 path on a sample with the same grid mix
+        sample = groups[:24]
+        plain = Engine(sample, path=BEC_PATH_FP64_PLAIN)
+        for g, d in enumerate(plain.derived):
+            plain.init_group(g, thomas_fermi(d))
+        plain.start_evolution()
+        plain.evolve(1)
+        plain.evolve(2)
+        pv = len(sample) * 2 / (plain.last_device_ms * 1e-3)
+        # the batched path on the same sample, for the like-for-like ratio
+        bs = Engine(sample, path=BEC_PATH_FP32_BATCHED)
+        for g, d in enumerate(bs.derived):
+            bs.init_group(g, thomas_fermi(d))
+        bs.start_evolution()
+        bs.evolve(3)
+        bs.evolve(10)
+        bv = len(sample) * 10 / (bs.last_device_ms * 1e-3)
+        extras["plain_fp64"] = {"value": pv, "unit": "traj-steps/s", "sample": f"{len(sample)} trajectories, 2 steps",
+                                "batched_fp32_same_sample": bv, "ratio_same_sample": bv / pv,
+                                "ratio_full_batch": value / pv}
+        plain.close()
+        bs.close()
+        v, cores, s = cpu_baseline(groups, args.cpu_seconds)
+        cpu = {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": s}
+
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": "wigner_traj_steps_per_s", "value": value, "unit": "traj-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD if not args.grids else f"{args.n_traj}x{args.grids}",
+                       "n_traj_per_gpu": args.n_traj,
+                       "grids": args.grids or "8x8x64/16x16x128/32x32x256 uniform", "N": "U[5000,70000]",
+                       "trap_jitter": "+-10%", "dt_s": 4e-5, "noise": "Philox vacuum + loss noise",
+                       "l2": f"state {16 * total_cells / 1e9:.2f} GB per GPU, larger than L2",
+                       "parallelism": f"dp{ws} (trajectory sharding)", "path": "fp32-batched"},
+            "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks, **extras,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

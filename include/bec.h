@@ -263,6 +263,17 @@ double bec_last_device_ms(const bec_ctx *ctx);
 /* Number of this library's kernel launches issued by the last bec_evolve / bec_run. */
 int64_t bec_last_launch_count(const bec_ctx *ctx);
 
+/* Runs n_steps real-time steps with CUDA events on the engine's stream around
+ * every launch and reports, per grid class c (batched path; on the plain path
+ * every group is a class): dims[3c..3c+2] = (nvx, nvy, nvz), traj[c] = its
+ * trajectory count, ms[2c] / ms[2c+1] = mean device time of one z-pass /
+ * plane-pass launch (plain path: ms[2c] = one trajectory-step, ms[2c+1] = 0).
+ * At most max_classes classes are written; *n_classes receives the count.
+ * No counterpart in the reference, which times with gettimeofday around whole
+ * steps (wigner.cpp:365-369). */
+bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes, int32_t *dims,
+                             int64_t *traj, double *ms, int32_t *n_classes);
+
 #ifdef __cplusplus
 }
 #endif

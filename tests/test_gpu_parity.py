@@ -185,7 +185,13 @@ def test_run_with_pi_pulse_and_axial(path):
     ax_e = axial[0][-1]
     # the last sample precedes nothing else, so it is the oracle's final state
     np.testing.assert_allclose(ax_e[:, :2], ax_o[:, :2], rtol=tol * 10, atol=tol * ax_o[:, :2].max())
-    np.testing.assert_allclose(OBS.axial_ratio(ax_e, eo.d, p.ne), eo.ref_axial_ratio(),
+    # the ratio (a - b)/(a + b) is ill-conditioned where the Wigner-subtracted density
+    # a + b vanishes (the condensate's edge); compare it where a + b is resolved
+    d = eo.d
+    sub = p.ne * d.nvx * d.nvy * d.V / 2.0
+    tot = ax_o[:, 0] + ax_o[:, 1] - 2 * sub
+    keep = np.abs(tot) > 0.05 * np.abs(tot).max()
+    np.testing.assert_allclose(OBS.axial_ratio(ax_e, d, p.ne)[keep], eo.ref_axial_ratio()[keep],
                                atol=1e-8 if path == BEC_PATH_FP64_PLAIN else 1e-3)
     obs = eng.observables(0, mom[-1, 0])
     assert obs["visibility_scan"] == pytest.approx(eo.ref_visibility(), abs=1e-9 if path == BEC_PATH_FP64_PLAIN else FP32_VIS)
