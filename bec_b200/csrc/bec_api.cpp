@@ -69,6 +69,8 @@ struct bec_ctx {
     std::vector<ClassRec> classes;
     std::map<int, double2 *> tw64;
     std::map<int, float2 *> tw32;
+    std::map<int, float2 *> tw32_full;
+    bool use_fast = true;                // register-resident passes where the shape allows
     GroupParamsF *d_gparams = nullptr;
     double *d_traj_tot = nullptr;        // [n_traj][4]
     double *d_group_mom = nullptr;       // [n_groups][4]
@@ -235,6 +237,24 @@ bec_status get_tw32(bec_ctx *ctx, int n, float2 **out)
     return BEC_OK;
 }
 
+// all n twiddles W_n^e, e < n (the pencil pass indexes products j * k1 < n)
+bec_status get_tw32_full(bec_ctx *ctx, int n, float2 **out)
+{
+    auto it = ctx->tw32_full.find(n);
+    if (it != ctx->tw32_full.end()) { *out = it->second; return BEC_OK; }
+    std::vector<float2> f(n);
+    for (int k = 0; k < n; ++k) {
+        double a = 2.0 * M_PI * (double)k / (double)n;
+        f[k] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    float2 *d = nullptr;
+    CKC(dalloc(ctx, &d, f.size()));
+    CKC(cudaMemcpy(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    ctx->tw32_full[n] = d;
+    *out = d;
+    return BEC_OK;
+}
+
 bec_status plain_fft(bec_ctx *ctx, double2 *data, const GeomD &g, int inv)
 {
     double2 *tx, *ty, *tz;
@@ -265,8 +285,9 @@ bec_status plain_step(bec_ctx *ctx, GroupRec &gr, int t)
 
 // ---------------------------------------------------------------- batched z pass
 // ends_step: no plane pass follows, so the pass leaves the state in the form a z pass reads
+// ev (optional): per class (start, stop) events recorded around that class's launch
 bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, const double2 *m2,
-                             bool ends_step = false)
+                             bool ends_step = false, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr)
 {
     ZPassArgs z{};
     z.pre = pre;
@@ -280,30 +301,60 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
         z.has_m2 = 1;
         for (int i = 0; i < 4; ++i) z.m2[i] = make_float2((float)m2[i].x, (float)m2[i].y);
     }
+    // without an observation the two pulse matrices collapse into one
+    float2 mfused[4];
+    const float2 *mf = nullptr;
+    if (!observe && (z.has_m1 || z.has_m2)) {
+        double2 a[4], b[4], r[4];
+        for (int i = 0; i < 4; ++i) {
+            a[i] = z.has_m2 ? m2[i] : cd(i == 0 || i == 3 ? 1.0 : 0.0, 0.0);
+            b[i] = z.has_m1 ? ctx->pulse[i] : cd(i == 0 || i == 3 ? 1.0 : 0.0, 0.0);
+        }
+        matmul2(a, b, r);
+        for (int i = 0; i < 4; ++i) mfused[i] = make_float2((float)r[i].x, (float)r[i].y);
+        mf = mfused;
+    }
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
-        float2 *tz;
         bec_status st;
-        if ((st = get_tw32(ctx, c.geom.nz, &tz))) return st;
         z.scale = (float)(1.0 / (double)c.geom.cells);
         z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
-        fp32_zpass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, tz, z, c.obs_partial, ctx->stream);
+        const size_t ci = &c - &ctx->classes[0];
+        if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
+        if (!observe && ctx->use_fast && fp32_fast_pencil_supported(c.geom)) {
+            float2 *twf;
+            if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
+            fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, pre + post, z.scale * z.out_scale,
+                             mf, ctx->stream);
+        } else {
+            float2 *tz;
+            if ((st = get_tw32(ctx, c.geom.nz, &tz))) return st;
+            fp32_zpass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, tz, z, c.obs_partial, ctx->stream);
+        }
+        if (ev) CKC(cudaEventRecord(ev[ci].second, ctx->stream));
         CKL();
     }
     ctx->has_pulse = false;
     return BEC_OK;
 }
 
-bec_status batched_ppass_all(bec_ctx *ctx)
+bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr)
 {
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
-        float2 *tx, *ty;
-        bec_status st;
-        if ((st = get_tw32(ctx, c.geom.nx, &tx))) return st;
-        if ((st = get_tw32(ctx, c.geom.ny, &ty))) return st;
-        fp32_ppass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, tx, ty, (uint32_t)ctx->step,
-                   ctx->stream);
+        const size_t ci = &c - &ctx->classes[0];
+        if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
+        if (ctx->use_fast && fp32_fast_plane_supported(c.geom)) {
+            fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, (uint32_t)ctx->step, ctx->stream);
+        } else {
+            float2 *tx, *ty;
+            bec_status st;
+            if ((st = get_tw32(ctx, c.geom.nx, &tx))) return st;
+            if ((st = get_tw32(ctx, c.geom.ny, &ty))) return st;
+            fp32_ppass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, tx, ty, (uint32_t)ctx->step,
+                       ctx->stream);
+        }
+        if (ev) CKC(cudaEventRecord(ev[ci].second, ctx->stream));
         CKL();
     }
     return BEC_OK;
@@ -1240,41 +1291,17 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
                 CKC(cudaEventRecord(mk.second, s));
             }
         } else {
-            ZPassArgs z{};
-            z.pre = ctx->pending ? 0.5f : 0.0f;
-            z.post = 0.5f;
-            z.out_scale = 1.0f;
-            if (ctx->has_pulse) {
-                z.has_m1 = 1;
-                for (int k = 0; k < 4; ++k) z.m1[k] = make_float2((float)ctx->pulse[k].x, (float)ctx->pulse[k].y);
-            }
+            std::vector<std::pair<cudaEvent_t, cudaEvent_t>> zev(nc), pev(nc);
             for (int c = 0; c < nc; ++c) {
-                ClassRec &cr = ctx->classes[c];
-                if (cr.geom.n_traj == 0) continue;
-                float2 *tz;
-                if ((st = get_tw32(ctx, cr.geom.nz, &tz))) return st;
-                z.scale = (float)(1.0 / (double)cr.geom.cells);
-                auto &mk = marks[((size_t)i * nc + c) * 2];
-                mk.first = new_event();
-                mk.second = new_event();
-                CKC(cudaEventRecord(mk.first, s));
-                fp32_zpass(cr.state, cr.geom, ctx->d_gparams, cr.d_tgroup, tz, z, cr.obs_partial, s);
-                CKC(cudaEventRecord(mk.second, s));
+                zev[c] = {new_event(), new_event()};
+                pev[c] = {new_event(), new_event()};
+                marks[((size_t)i * nc + c) * 2] = zev[c];
+                marks[((size_t)i * nc + c) * 2 + 1] = pev[c];
             }
-            ctx->has_pulse = false;
+            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr, false, zev.data())))
+                return st;
             ctx->pending = true;
-            for (int c = 0; c < nc; ++c) {
-                ClassRec &cr = ctx->classes[c];
-                if (cr.geom.n_traj == 0) continue;
-                float2 *tx, *ty;
-                if ((st = get_tw32(ctx, cr.geom.nx, &tx)) || (st = get_tw32(ctx, cr.geom.ny, &ty))) return st;
-                auto &mk = marks[((size_t)i * nc + c) * 2 + 1];
-                mk.first = new_event();
-                mk.second = new_event();
-                CKC(cudaEventRecord(mk.first, s));
-                fp32_ppass(cr.state, cr.geom, ctx->d_gparams, cr.d_tgroup, cr.d_tlocal, tx, ty, (uint32_t)ctx->step, s);
-                CKC(cudaEventRecord(mk.second, s));
-            }
+            if ((st = batched_ppass_all(ctx, pev.data()))) return st;
         }
         CKL();
         ctx->step++;

@@ -111,3 +111,13 @@ void group_reduce(const double *traj_tot, const int *group_first, const int *gro
 
 // launch counter (kernels this library enqueued since the counter was reset)
 extern thread_local long long g_launches;
+
+// fused_passes.cu: register-resident passes (square planes 8/16/32; nz = 64/128/256)
+bool fp32_fast_plane_supported(const ClassGeom &c);
+bool fp32_fast_pencil_supported(const ClassGeom &c);
+void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
+                     uint32_t step, cudaStream_t s);
+// tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times the output scale;
+// m: optional pulse matrix (row-major, 4 entries) or NULL
+void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
+                      const float2 *tw_full, float frac, float scale, const float2 *m, cudaStream_t s);

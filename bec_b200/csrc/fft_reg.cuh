@@ -1,0 +1,142 @@
+// fft_reg.cuh -- register-resident DFTs of compile-time size.
+//
+// A thread holds a whole line (N <= 32 elements) in registers; the DFT is a
+// fully unrolled radix-2 Cooley-Tukey recursion whose twiddles are
+// compile-time constants, so trivial twiddles (1, -i, +i) cost nothing and
+// the rest become FMA immediates. Elements are float2 (one complex value) or
+// float4 (the two components a, b of one cell, transformed together).
+//
+// Twiddle values come from cos_2pi / sin_2pi below: exact octant reduction on the
+// integer angle 2 pi k / n, then Taylor series on [0, pi/2) in double
+// precision (error ~1e-16), evaluated by the compiler.
+#pragma once
+
+#include <utility>
+
+#include "common.cuh"
+
+namespace fftreg {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+__host__ __device__ constexpr double taylor_sin(double x)
+{
+    double t = x, s = x;
+    for (int i = 1; i < 24; ++i) {
+        t *= -x * x / ((2.0 * i) * (2.0 * i + 1.0));
+        s += t;
+    }
+    return s;
+}
+
+__host__ __device__ constexpr double taylor_cos(double x)
+{
+    double t = 1.0, s = 1.0;
+    for (int i = 1; i < 24; ++i) {
+        t *= -x * x / ((2.0 * i - 1.0) * (2.0 * i));
+        s += t;
+    }
+    return s;
+}
+
+// cos(2 pi k / n) and sin(2 pi k / n) for integer k, n > 0
+__host__ __device__ constexpr double cos_2pi(long k, long n)
+{
+    k %= n;
+    if (k < 0) k += n;
+    const long q = (4 * k) / n, r = 4 * k - q * n;
+    const double a = (kPi / 2.0) * (double)r / (double)n;
+    const double sa = taylor_sin(a), ca = taylor_cos(a);
+    return q == 0 ? ca : q == 1 ? -sa : q == 2 ? -ca : sa;
+}
+
+__host__ __device__ constexpr double sin_2pi(long k, long n)
+{
+    k %= n;
+    if (k < 0) k += n;
+    const long q = (4 * k) / n, r = 4 * k - q * n;
+    const double a = (kPi / 2.0) * (double)r / (double)n;
+    const double sa = taylor_sin(a), ca = taylor_cos(a);
+    return q == 0 ? sa : q == 1 ? ca : q == 2 ? -sa : -ca;
+}
+
+// ---- element operations ----------------------------------------------------
+__device__ __forceinline__ float2 add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float4 add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+
+// v * (c + i s)
+__device__ __forceinline__ float2 cmulc(float2 v, float c, float s)
+{
+    return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+}
+__device__ __forceinline__ float4 cmulc(float4 v, float c, float s)
+{
+    return make_float4(v.x * c - v.y * s, v.x * s + v.y * c, v.z * c - v.w * s, v.z * s + v.w * c);
+}
+// v * (-i)
+__device__ __forceinline__ float2 mul_negi(float2 v) { return make_float2(v.y, -v.x); }
+__device__ __forceinline__ float4 mul_negi(float4 v) { return make_float4(v.y, -v.x, v.w, -v.z); }
+// v * (+i)
+__device__ __forceinline__ float2 mul_posi(float2 v) { return make_float2(-v.y, v.x); }
+__device__ __forceinline__ float4 mul_posi(float4 v) { return make_float4(-v.y, v.x, -v.w, v.z); }
+
+// v * w with w a runtime complex (float2)
+__device__ __forceinline__ float2 cmulw(float2 v, float2 w) { return make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x); }
+__device__ __forceinline__ float4 cmulw(float4 v, float2 w)
+{
+    return make_float4(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x, v.z * w.x - v.w * w.y, v.z * w.y + v.w * w.x);
+}
+
+// ---- DFT ---------------------------------------------------------------------
+// x[k] <- sum_n x[n] exp(-+2 pi i n k / N) (sign - forward, + when INV), unnormalised.
+template <int N, bool INV, typename T>
+__device__ __forceinline__ void dft(T *x);
+
+template <int N, bool INV, int K, typename T>
+__device__ __forceinline__ void combine_one(T *x, const T *e, const T *o)
+{
+    T t;
+    if constexpr (K == 0) {
+        t = o[K];
+    } else if constexpr (4 * K == N) {
+        t = INV ? mul_posi(o[K]) : mul_negi(o[K]);
+    } else {
+        constexpr double c = cos_2pi(K, N);
+        constexpr double s = sin_2pi(K, N);
+        t = cmulc(o[K], (float)c, INV ? (float)s : -(float)s);
+    }
+    x[K] = add(e[K], t);
+    x[K + N / 2] = sub(e[K], t);
+}
+
+template <int N, bool INV, typename T, int... K>
+__device__ __forceinline__ void combine_all(T *x, const T *e, const T *o, std::integer_sequence<int, K...>)
+{
+    (combine_one<N, INV, K>(x, e, o), ...);
+}
+
+template <int N, bool INV, typename T>
+__device__ __forceinline__ void dft(T *x)
+{
+    if constexpr (N == 1) {
+        return;
+    } else if constexpr (N == 2) {
+        const T a = x[0], b = x[1];
+        x[0] = add(a, b);
+        x[1] = sub(a, b);
+    } else {
+        T e[N / 2], o[N / 2];
+#pragma unroll
+        for (int k = 0; k < N / 2; ++k) {
+            e[k] = x[2 * k];
+            o[k] = x[2 * k + 1];
+        }
+        dft<N / 2, INV>(e);
+        dft<N / 2, INV>(o);
+        combine_all<N, INV>(x, e, o, std::make_integer_sequence<int, N / 2>{});
+    }
+}
+
+} // namespace fftreg

@@ -1,0 +1,269 @@
+// fused_passes.cu -- register-resident plane and pencil passes of the FP32 path.
+//
+// Same two-pass regrouping of the reference's split step as batched_fp32.cu
+// (propagate, programs/bec_wigner_3d.cuda/wigner.cu:178-199) and the same
+// stored representation, but every line of the 3D transform lives in one
+// thread's registers and shared memory is used only to transpose:
+//
+// plane pass (square planes N x N, N = 8, 16, 32): one warp per 32/N planes.
+//   lane c loads column c of its plane straight from HBM (each load instruction
+//   of the warp reads consecutive 16-byte cells), transforms it along y, writes
+//   it to an XOR-swizzled shared tile, reads back row c, transforms along x,
+//   applies the nonlinear / loss / loss-noise step to its N cells, and returns
+//   the same way. Both components of a cell are one float4.
+//
+// pencil pass (nz = 64, 128, 256 = 16 G): one CTA per 16 adjacent pencils of a
+//   trajectory, 16 G threads. A four-step decomposition nz = 16 x G: each
+//   thread holds 16 elements (z = j + G m) and does a 16-point DFT, twiddles,
+//   and after one shared-memory transpose a G-point DFT across j; the kinetic
+//   phase e^{i k^2/2 dt} (wigner_kernel.cu:137-151) is applied in full k-space
+//   as the product of a per-pencil (kx, ky) factor and a per-kz factor; the
+//   forward transform retraces the same steps.
+//
+// Shared tiles are swizzled on the 16-byte unit index (col ^ (row & 7)) so
+// that both the row-wise and the column-wise access of a quarter warp touch
+// eight different bank groups.
+#include "engine.h"
+#include "fft_reg.cuh"
+#include "physics.cuh"
+
+namespace {
+
+using fftreg::dft;
+
+// ---------------------------------------------------------------- plane pass
+template <int N>
+__global__ void __launch_bounds__(128) k_plane(float4 *__restrict__ state, int nz, int cells,
+                                               const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
+                                               const int *__restrict__ tlocal, uint32_t step)
+{
+    constexpr int W = 32 / N;          // planes per warp
+    constexpr int PLANE = N * N;
+    extern __shared__ float4 tile[];   // 4 warps x W planes x PLANE
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wp = lane / N, c = lane % N;
+    const int plane_id = (blockIdx.x * 4 + warp) * W + wp;
+    const int traj = plane_id / nz, z = plane_id - traj * nz;
+    float4 *__restrict__ g = state + (size_t)traj * cells + (size_t)z * PLANE;
+    float4 *s = tile + (warp * W + wp) * PLANE;
+
+    float4 v[N];
+#pragma unroll
+    for (int y = 0; y < N; ++y) v[y] = g[y * N + c];
+    dft<N, false>(v);                                  // along y: k_y -> y
+#pragma unroll
+    for (int y = 0; y < N; ++y) s[y * N + (c ^ (y & 7))] = v[y];
+    __syncwarp();
+#pragma unroll
+    for (int x = 0; x < N; ++x) v[x] = s[c * N + (x ^ (c & 7))];
+    dft<N, false>(v);                                  // along x: k_x -> x; lane c holds row y = c
+
+    const GroupParamsF P = gp[tgroup[traj]];
+    const float Y = -P.ymax + P.dy * (float)c;
+    const float Z = -P.zmax + P.dz * (float)z;
+    const float base = Y * Y + Z * Z * P.inv_lambda2;
+    const uint32_t tl = (uint32_t)tlocal[traj];
+    const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+        const float X = -P.xmax + P.dx * (float)x;
+        const float V = 0.5f * (X * X + base);
+        const float4 v0 = v[x];
+        float4 o = nonlinear_cell(v0, V, P);
+        if (P.noise) o = loss_noise_cell(o, v0, P, tl, step, cell0 + x);
+        v[x] = o;
+    }
+
+    dft<N, true>(v);                                   // x -> k_x (unnormalised)
+#pragma unroll
+    for (int x = 0; x < N; ++x) s[c * N + (x ^ (c & 7))] = v[x];
+    __syncwarp();
+#pragma unroll
+    for (int y = 0; y < N; ++y) v[y] = s[y * N + (c ^ (y & 7))];
+    dft<N, true>(v);                                   // y -> k_y (unnormalised)
+#pragma unroll
+    for (int y = 0; y < N; ++y) g[y * N + c] = v[y];
+}
+
+// ---------------------------------------------------------------- pencil pass
+struct PencilArgs {
+    float frac;          // kick in units of dt (0.5 + 0.5 for a full step)
+    float scale;         // 1/cells times the output scale
+    int has_m;
+    float2 m[4];         // pulse matrix, row-major
+};
+
+template <int NZ>
+__global__ void __launch_bounds__(NZ) k_pencil(float4 *__restrict__ state, int nx, int lx, int ny, int cells,
+                                               int tiles, const GroupParamsF *__restrict__ gp,
+                                               const int *__restrict__ tgroup, const float2 *__restrict__ tw_g,
+                                               PencilArgs pa)
+{
+    constexpr int R = 16, G = NZ / 16;
+    extern __shared__ float4 dyn[];
+    float4 *buf = dyn;                                          // 16 pencils x NZ
+    float2 *tw = reinterpret_cast<float2 *>(dyn + 16 * NZ);     // W_NZ^e, e < NZ
+    float2 *kzp = tw + NZ;                                      // kz phase
+    float2 *kxyp = kzp + NZ;                                    // (kx, ky) phase x scale, per pencil
+
+    const int t = threadIdx.x;
+    const int traj = blockIdx.x / tiles;
+    const int pen0 = (blockIdx.x - traj * tiles) * 16;
+    const GroupParamsF P = gp[tgroup[traj]];
+    const int plane = nx * ny;
+
+    for (int i = t; i < NZ; i += blockDim.x) {
+        tw[i] = tw_g[i];
+        const float kz = getk<float>(i, P.dkz, NZ);
+        float s, c;
+        sincosf(0.5f * kz * kz * P.dt * pa.frac, &s, &c);      // e^{+i k^2/2 dt frac}
+        kzp[i] = make_float2(c, s);
+    }
+    if (t < 16) {
+        const int pen = pen0 + t;
+        const int x = pen & (nx - 1), y = pen >> lx;
+        const float kx = getk<float>(x, P.dkx, nx);
+        const float ky = (ny > 1) ? getk<float>(y, P.dky, ny) : 0.0f;
+        float s, c;
+        sincosf(0.5f * (kx * kx + ky * ky) * P.dt * pa.frac, &s, &c);
+        kxyp[t] = make_float2(pa.scale * c, pa.scale * s);
+    }
+
+    // stage 1: thread (p, j) holds z = j + G m, m < 16
+    const int p = t & 15, j = t >> 4;
+    float4 *__restrict__ g = state + (size_t)traj * cells + pen0 + p;
+    float4 x[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) x[m] = g[(size_t)(j + G * m) * plane];
+    __syncthreads();                                            // tables ready
+    dft<R, true>(x);                                            // over m -> k1 (inverse)
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) {
+        const float2 w = tw[j * k1];
+        x[k1] = fftreg::cmulw(x[k1], make_float2(w.x, -w.y));   // W^{-j k1}
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[(p * G + j) * R + (k1 ^ (p & 7))] = x[k1];
+    __syncthreads();
+
+    // stage 2: thread (q, p2) holds k1 = q + G r (r < 16/G) for all j, then all k2
+    const int q = t % G, p2 = t / G;
+    float4 y[R];
+#pragma unroll
+    for (int r = 0; r < R / G; ++r)
+#pragma unroll
+        for (int jj = 0; jj < G; ++jj) y[r * G + jj] = buf[(p2 * G + jj) * R + ((q + G * r) ^ (p2 & 7))];
+#pragma unroll
+    for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);   // over j -> k2: k = k1 + 16 k2
+
+    const float2 pxy = kxyp[p2];
+#pragma unroll
+    for (int r = 0; r < R / G; ++r)
+#pragma unroll
+        for (int k2 = 0; k2 < G; ++k2) {
+            const int k = q + G * r + R * k2;
+            float4 v = fftreg::cmulw(y[r * G + k2], cmul(pxy, kzp[k]));
+            if (pa.has_m) {
+                const float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
+                const float2 an = cadd(cmul(pa.m[0], a), cmul(pa.m[1], b));
+                const float2 bn = cadd(cmul(pa.m[2], a), cmul(pa.m[3], b));
+                v = make_float4(an.x, an.y, bn.x, bn.y);
+            }
+            y[r * G + k2] = v;
+        }
+
+#pragma unroll
+    for (int r = 0; r < R / G; ++r) dft<G, false>(y + r * G); // over k2 -> j (forward)
+#pragma unroll
+    for (int r = 0; r < R / G; ++r)
+#pragma unroll
+        for (int jj = 1; jj < G; ++jj) y[r * G + jj] = fftreg::cmulw(y[r * G + jj], tw[(q + G * r) * jj]);
+    __syncthreads();                                            // stage-2 reads done
+#pragma unroll
+    for (int r = 0; r < R / G; ++r)
+#pragma unroll
+        for (int jj = 0; jj < G; ++jj) buf[(p2 * G + jj) * R + ((q + G * r) ^ (p2 & 7))] = y[r * G + jj];
+    __syncthreads();
+
+    // stage 3: thread (p, j) gathers k1 < 16 and finishes over k1 -> m
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[(p * G + j) * R + (k1 ^ (p & 7))];
+    dft<R, false>(x);
+#pragma unroll
+    for (int m = 0; m < R; ++m) g[(size_t)(j + G * m) * plane] = x[m];
+}
+
+template <int NZ>
+void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const float2 *tw,
+                   const PencilArgs &pa, cudaStream_t s)
+{
+    const int tiles = c.nx * c.ny / 16;
+    const size_t smem = sizeof(float4) * 16 * NZ + sizeof(float2) * (2 * NZ + 16);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_pencil<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_pencil<NZ><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, tgroup, tw, pa);
+    g_launches++;
+}
+
+template <int N>
+void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
+                  uint32_t step, cudaStream_t s)
+{
+    constexpr int W = 32 / N;
+    const int planes = c.n_traj * c.nz;
+    const size_t smem = sizeof(float4) * 4 * W * N * N;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_plane<N><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
+    g_launches++;
+}
+
+} // namespace
+
+bool fp32_fast_plane_supported(const ClassGeom &c)
+{
+    if (c.nx != c.ny || (c.nx != 8 && c.nx != 16 && c.nx != 32)) return false;
+    const int W = 32 / c.nx;
+    return ((long long)c.n_traj * c.nz) % (4 * W) == 0;
+}
+
+bool fp32_fast_pencil_supported(const ClassGeom &c)
+{
+    return (c.nz == 64 || c.nz == 128 || c.nz == 256) && (c.nx * c.ny) % 16 == 0 && c.nx * c.ny >= 16;
+}
+
+void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
+                     uint32_t step, cudaStream_t s)
+{
+    if (c.n_traj <= 0) return;
+    switch (c.nx) {
+    case 8: launch_plane<8>(state, c, gp, tgroup, tlocal, step, s); break;
+    case 16: launch_plane<16>(state, c, gp, tgroup, tlocal, step, s); break;
+    case 32: launch_plane<32>(state, c, gp, tgroup, tlocal, step, s); break;
+    default: break;
+    }
+}
+
+void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
+                      const float2 *tw_full, float frac, float scale, const float2 *m, cudaStream_t s)
+{
+    if (c.n_traj <= 0) return;
+    PencilArgs pa{};
+    pa.frac = frac;
+    pa.scale = scale;
+    pa.has_m = m ? 1 : 0;
+    if (m)
+        for (int i = 0; i < 4; ++i) pa.m[i] = m[i];
+    switch (c.nz) {
+    case 64: launch_pencil<64>(state, c, gp, tgroup, tw_full, pa, s); break;
+    case 128: launch_pencil<128>(state, c, gp, tgroup, tw_full, pa, s); break;
+    case 256: launch_pencil<256>(state, c, gp, tgroup, tw_full, pa, s); break;
+    default: break;
+    }
+}

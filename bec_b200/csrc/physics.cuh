@@ -1,0 +1,81 @@
+// physics.cuh -- the per-cell real-space step of the FP32 path, shared by the
+// plane-pass kernels.
+//
+// propagateXSpaceTwoComponent (programs/bec_wigner_3d.cuda/wigner_kernel.cu:184-229):
+// itmax midpoint iterations of the exponential integrator
+//   pa = -(l111 na^2 + l12 nb)/2 + i (V + g11 na + g12 nb)
+//   pb = -(l22 nb + l12 na)/2  + i (V + g22 nb + g12 na - detuning)
+//   d  = exp(p dt/2),  psi = psi0 d  (x itmax),  out = psi d
+// (the reference's sign: evolution by e^{+i H dt}, wigner_kernel.cu:206-215),
+// followed by the Wigner loss-noise increment at the start of the substep:
+//   a += 3 sqrt(l111/6) conj(a0)^2 dW1 + sqrt(l12/2) conj(b0) dW2
+//   b +=   sqrt(l12/2)  conj(a0)   dW2 + sqrt(l22)   conj(b0) dW3,
+// dW complex normal with <|dW|^2> = dt / dV, drawn from Philox4x32-10 keyed by
+// the ensemble seed with counter (cell, step, trajectory, channel tag).
+#pragma once
+
+#include "common.cuh"
+#include "engine.h"
+
+// Box-Muller with the SFU log/sin/cos: ~1e-6 relative agreement with the
+// FP64 draws of the oracle for the same counter.
+__device__ __forceinline__ void box_muller_fast(uint32_t x1, uint32_t x2, float &n1, float &n2)
+{
+    const float u1 = fmaf((float)x1, 0x1p-32f, 0x1p-32f);       // (x1 + 1) / 2^32 in (0, 1]
+    const float r = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f));
+    float s, c;
+    __sincosf(6.28318530717958648f * ((float)x2 * 0x1p-32f), &s, &c);
+    n1 = r * c;
+    n2 = r * s;
+}
+
+__device__ __forceinline__ void normals4_fast(uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
+                                              uint32_t cell, uint32_t tag, float out[4])
+{
+    const u32x4 r = philox4x32_10(cell, step, traj, tag, k0, k1);
+    box_muller_fast(r.x, r.y, out[0], out[1]);
+    box_muller_fast(r.z, r.w, out[2], out[3]);
+}
+
+// One cell: v = (a, b) at the start of the substep, V the trap potential.
+__device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupParamsF &P)
+{
+    const float2 a0 = make_float2(v.x, v.y), b0 = make_float2(v.z, v.w);
+    const float hdt = P.dt * 0.5f;
+    float2 xa = a0, xb = b0, da = make_float2(0.f, 0.f), db = make_float2(0.f, 0.f);
+    for (int it = 0; it < P.itmax; ++it) {
+        const float na = xa.x * xa.x + xa.y * xa.y;
+        const float nb = xb.x * xb.x + xb.y * xb.y;
+        const float pa_re = -(P.l111 * na * na + P.l12 * nb) * 0.5f;
+        const float pa_im = V + P.g11 * na + P.g12 * nb;
+        const float pb_re = -(P.l22 * nb + P.l12 * na) * 0.5f;
+        const float pb_im = V + P.g22 * nb + P.g12 * na - P.detuning;
+        float sa, ca, sb, cb;
+        sincosf(pa_im * hdt, &sa, &ca);
+        sincosf(pb_im * hdt, &sb, &cb);
+        const float ma = expf(pa_re * hdt), mb = expf(pb_re * hdt);
+        da = make_float2(ma * ca, ma * sa);
+        db = make_float2(mb * cb, mb * sb);
+        xa = cmul(a0, da);
+        xb = cmul(b0, db);
+    }
+    const float2 ao = cmul(xa, da), bo = cmul(xb, db);
+    return make_float4(ao.x, ao.y, bo.x, bo.y);
+}
+
+// Adds the loss-noise increment evaluated at v0 to out.
+__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const GroupParamsF &P, uint32_t traj,
+                                                  uint32_t step, uint32_t cell)
+{
+    float r1[4], r2[4];
+    normals4_fast(P.seed_lo, P.seed_hi, traj, step, cell, RNG_TAG_LOSS1, r1);
+    normals4_fast(P.seed_lo, P.seed_hi, traj, step, cell, RNG_TAG_LOSS2, r2);
+    const float s = P.noise_amp;
+    const float2 w1 = make_float2(s * r1[0], s * r1[1]);
+    const float2 w2 = make_float2(s * r1[2], s * r1[3]);
+    const float2 w3 = make_float2(s * r2[0], s * r2[1]);
+    const float2 ca = make_float2(v0.x, -v0.y), cb = make_float2(v0.z, -v0.w);
+    const float2 da = cadd(cmul(cscale(cmul(ca, ca), P.c1), w1), cmul(cscale(cb, P.c2), w2));
+    const float2 db = cadd(cmul(cscale(ca, P.c2), w2), cmul(cscale(cb, P.c3), w3));
+    return make_float4(out.x + da.x, out.y + da.y, out.z + db.x, out.w + db.y);
+}

@@ -257,7 +257,7 @@ def main():
     for c in prof:
         nx, ny, nz = c["dims"]
         bytes_launch = 32.0 * nx * ny * nz * c["traj"]      # read + write of both complex64 components
-        for kind, t in (("zpass", c["z_ms"]), ("ppass", c["plane_ms"])):
+        for kind, t in (("pencil", c["z_ms"]), ("plane", c["plane_ms"])):
             kernels.append(dict(kernel=f"{kind}_{nx}x{ny}x{nz}", ms=t, bytes=bytes_launch, traj=c["traj"]))
     dom = max(kernels, key=lambda k: k["ms"])
     achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
