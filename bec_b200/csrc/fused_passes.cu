@@ -33,7 +33,7 @@ using fftreg::dft;
 
 // ---------------------------------------------------------------- plane pass
 template <int N>
-__global__ void __launch_bounds__(128) k_plane(float4 *__restrict__ state, int nz, int cells,
+__global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, int nz, int cells,
                                                const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
                                                const int *__restrict__ tlocal, uint32_t step)
 {
@@ -47,40 +47,65 @@ __global__ void __launch_bounds__(128) k_plane(float4 *__restrict__ state, int n
     float4 *__restrict__ g = state + (size_t)traj * cells + (size_t)z * PLANE;
     float4 *s = tile + (warp * W + wp) * PLANE;
 
+    const GroupParamsF P = gp[tgroup[traj]];
+
     float4 v[N];
 #pragma unroll
     for (int y = 0; y < N; ++y) v[y] = g[y * N + c];
-    dft<N, false>(v);                                  // along y: k_y -> y
-#pragma unroll
-    for (int y = 0; y < N; ++y) s[y * N + (c ^ (y & 7))] = v[y];
-    __syncwarp();
-#pragma unroll
-    for (int x = 0; x < N; ++x) v[x] = s[c * N + (x ^ (c & 7))];
-    dft<N, false>(v);                                  // along x: k_x -> x; lane c holds row y = c
 
-    const GroupParamsF P = gp[tgroup[traj]];
-    const float Y = -P.ymax + P.dy * (float)c;
-    const float Z = -P.zmax + P.dz * (float)z;
-    const float base = Y * Y + Z * Z * P.inv_lambda2;
-    const uint32_t tl = (uint32_t)tlocal[traj];
-    const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
+    // Four transforms share one code body (the kernel is otherwise bound by
+    // instruction fetch): pass 0 forward along y, pass 1 forward along x,
+    // passes 2 and 3 inverse along x and y through IFFT(v) = conj(FFT(conj v)).
+#pragma unroll 1
+    for (int pass = 0; pass < 4; ++pass) {
+        const bool inv = pass >= 2;
+        if (inv) {
 #pragma unroll
-    for (int x = 0; x < N; ++x) {
-        const float X = -P.xmax + P.dx * (float)x;
-        const float V = 0.5f * (X * X + base);
-        const float4 v0 = v[x];
-        float4 o = nonlinear_cell(v0, V, P);
-        if (P.noise) o = loss_noise_cell(o, v0, P, tl, step, cell0 + x);
-        v[x] = o;
+            for (int i = 0; i < N; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
+        }
+        dft<N, false>(v);
+        if (inv) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
+        }
+        if (pass == 0) {
+            // column c -> row c
+#pragma unroll
+            for (int y = 0; y < N; ++y) s[y * N + (c ^ (y & 7))] = v[y];
+            __syncwarp();
+#pragma unroll
+            for (int x = 0; x < N; ++x) v[x] = s[c * N + (x ^ (c & 7))];
+        } else if (pass == 1) {
+            // lane c owns row y = c: the cells go through the physics one at a time
+            // from its own shared row (a rolled loop keeps the kernel small)
+#pragma unroll
+            for (int x = 0; x < N; ++x) s[c * N + (x ^ (c & 7))] = v[x];
+            const float Y = -P.ymax + P.dy * (float)c;
+            const float Z = -P.zmax + P.dz * (float)z;
+            const float base = Y * Y + Z * Z * P.inv_lambda2;
+            const uint32_t tl = (uint32_t)tlocal[traj];
+            const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
+#pragma unroll 1
+            for (int x = 0; x < N; ++x) {
+                const float X = -P.xmax + P.dx * (float)x;
+                const float V = 0.5f * (X * X + base);
+                float4 *slot = s + c * N + (x ^ (c & 7));
+                const float4 v0 = *slot;
+                float4 o = nonlinear_cell(v0, V, P);
+                if (P.noise) o = loss_noise_cell(o, v0, P, tl, step, cell0 + x);
+                *slot = o;
+            }
+#pragma unroll
+            for (int x = 0; x < N; ++x) v[x] = s[c * N + (x ^ (c & 7))];
+        } else if (pass == 2) {
+            // row c -> column c
+#pragma unroll
+            for (int x = 0; x < N; ++x) s[c * N + (x ^ (c & 7))] = v[x];
+            __syncwarp();
+#pragma unroll
+            for (int y = 0; y < N; ++y) v[y] = s[y * N + (c ^ (y & 7))];
+        }
     }
-
-    dft<N, true>(v);                                   // x -> k_x (unnormalised)
-#pragma unroll
-    for (int x = 0; x < N; ++x) s[c * N + (x ^ (c & 7))] = v[x];
-    __syncwarp();
-#pragma unroll
-    for (int y = 0; y < N; ++y) v[y] = s[y * N + (c ^ (y & 7))];
-    dft<N, true>(v);                                   // y -> k_y (unnormalised)
 #pragma unroll
     for (int y = 0; y < N; ++y) g[y * N + c] = v[y];
 }
