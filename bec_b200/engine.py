@@ -52,6 +52,8 @@ SIGNATURES = {
     "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
     "bec_profile_steps": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P(C.c_int32), _P(C.c_int64), _dp,
                                     _P(C.c_int32)]),
+    "bec_moments_device_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,
+                                             C.c_void_p]),
 }
 
 

@@ -274,6 +274,36 @@ int64_t bec_last_launch_count(const bec_ctx *ctx);
 bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes, int32_t *dims,
                              int64_t *traj, double *ms, int32_t *n_classes);
 
+/* ---- moments without device allocation -------------------------------- */
+
+/* Largest ne * cells accepted by bec_moments_device_noalloc. */
+#define BEC_NOALLOC_MAX_ELEMENTS 1073741824
+
+/*
+ * FP64 moments (na, nb, Re s, Im s), as in bec_moments, of ne x-space
+ * trajectories that already live in the caller's device memory:
+ *   d_psi: ne * 2 * cells interleaved complex doubles laid out [traj][a|b][cell];
+ *   d_out: 4 doubles of device memory receiving sum |a|^2 dV, sum |b|^2 dV and
+ *          the real and imaginary parts of sum conj(a) b dV over all trajectories;
+ *   stream: a cudaStream_t, or NULL for the default stream. The call only
+ *          enqueues work: synchronise the stream before reading d_out.
+ * No counterpart in the reference. It exists for callers that cannot let a
+ * library call cudaMalloc: hosts whose device memory all comes from their own
+ * pool, and loops that must never block on an allocation (cudaMalloc and
+ * cudaFree synchronise the device and can fail mid-run). It allocates nothing:
+ * the reduction's partial sums live in a fixed 64 KiB array that is part of the
+ * library image (every GPU that loads the library holds it until the process
+ * exits). The first call on a device looks up that array's device address, so
+ * make one call on each device before capturing any stream. All calls share
+ * the array: calls that overlap on the GPU (different streams, or several host
+ * threads) race and must be serialised by the caller; each call rewrites every
+ * partial sum it reads, so nothing carries over from the previous call.
+ * Returns BEC_ERR_INVALID_ARG for null pointers, non-positive sizes or dV, and
+ * for ne * cells above BEC_NOALLOC_MAX_ELEMENTS.
+ */
+bec_status bec_moments_device_noalloc(const double *d_psi, int32_t cells, int32_t ne, double dV,
+                                      double *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
