@@ -25,9 +25,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# ncu: DRAM bytes (read + write) per launch of the dominant kernel, measured on a
-# 64-trajectory 32x32x256 class (profiles/ppass_32x32x256.md), per trajectory.
-NCU_TRAFFIC_PER_TRAJ = None
+# ncu: DRAM bytes (read + write) of one launch divided by its trajectory count,
+# from captures of a 64-trajectory 32x32x256 class (profiles/plane_32x32x256.md,
+# profiles/pencil_32x32x256.md); traffic scales with the trajectories a launch
+# processes. Algorithmic: 32 B x 262144 cells = 8.39 MB per trajectory.
+NCU_TRAFFIC_PER_TRAJ = {
+    "plane_32x32x256": (268.494336e6 + 216.722688e6) / 64,
+    "pencil_32x32x256": (268.494592e6 + 214.559488e6) / 64,
+}
 
 N_TRAJ = 1024
 WORKLOAD = "uneven-ensembles-1024"
