@@ -76,7 +76,7 @@ class BecDerived(C.Structure):
 class BecGsOpts(C.Structure):
     _fields_ = [
         ("mode", C.c_int32), ("max_steps", C.c_int32), ("check_every", C.c_int32),
-        ("reserved", C.c_int32),
+        ("warm_per_group", C.c_int32),
         ("tol", C.c_double),
         ("warm_start", C.POINTER(C.c_double)),
     ]

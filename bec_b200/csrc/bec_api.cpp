@@ -55,7 +55,8 @@ struct ClassRec {
     double *d_traj_scale = nullptr;
     double *obs_partial = nullptr;
     double *traj_axial = nullptr;
-    int tiles = 1;
+    int tiles = 1;            // tiles per trajectory of the generic z pass
+    int obs_tiles = 1;        // tiles of the pass that last wrote obs_partial
     int traj_offset = 0;      // global index of the class's first trajectory
     std::vector<int> groups;  // group indices in this class
 };
@@ -304,7 +305,7 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
     // without an observation the two pulse matrices collapse into one
     float2 mfused[4];
     const float2 *mf = nullptr;
-    if (!observe && (z.has_m1 || z.has_m2)) {
+    if ((!observe && (z.has_m1 || z.has_m2)) || (observe && z.has_m1 && !z.has_m2)) {
         double2 a[4], b[4], r[4];
         for (int i = 0; i < 4; ++i) {
             a[i] = z.has_m2 ? m2[i] : cd(i == 0 || i == 3 ? 1.0 : 0.0, 0.0);
@@ -321,15 +322,20 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
         z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
         const size_t ci = &c - &ctx->classes[0];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
-        if (!observe && ctx->use_fast && fp32_fast_pencil_supported(c.geom)) {
+        // the register pencil pass observes only when it also ends the step (post = 0)
+        const bool fast = ctx->use_fast && fp32_fast_pencil_supported(c.geom) &&
+                          (!observe || (post == 0.0f && ends_step && !z.has_m2));
+        if (fast) {
             float2 *twf;
             if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
             fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, pre + post, z.scale * z.out_scale,
-                             mf, ctx->stream);
+                             mf, observe ? c.obs_partial : nullptr, z.out_scale, ctx->stream);
+            if (observe) c.obs_tiles = fp32_fast_pencil_tiles(c.geom);
         } else {
             float2 *tz;
             if ((st = get_tw32(ctx, c.geom.nz, &tz))) return st;
             fp32_zpass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, tz, z, c.obs_partial, ctx->stream);
+            if (observe) c.obs_tiles = c.tiles;
         }
         if (ev) CKC(cudaEventRecord(ev[ci].second, ctx->stream));
         CKL();
@@ -365,7 +371,7 @@ bec_status batched_reduce_obs(bec_ctx *ctx)
 {
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
-        obs_reduce(c.obs_partial, c.geom.n_traj, c.tiles, c.geom.nz, c.d_traj_scale, c.traj_axial,
+        obs_reduce(c.obs_partial, c.geom.n_traj, c.obs_tiles, c.geom.nz, c.d_traj_scale, c.traj_axial,
                    ctx->d_traj_tot + (size_t)c.traj_offset * 4, ctx->stream);
         CKL();
     }
@@ -686,7 +692,8 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
             CKA(dalloc(ctx, &c.d_tgroup, nt));
             CKA(dalloc(ctx, &c.d_tlocal, nt));
             CKA(dalloc(ctx, &c.d_traj_scale, nt));
-            CKA(dalloc(ctx, &c.obs_partial, nt * c.tiles * c.geom.nz * 4));
+            const int obs_cap = std::max(c.tiles, fp32_fast_pencil_supported(c.geom) ? fp32_fast_pencil_tiles(c.geom) : 1);
+            CKA(dalloc(ctx, &c.obs_partial, nt * obs_cap * c.geom.nz * 4));
             CKA(dalloc(ctx, &c.traj_axial, nt * c.geom.nz * 4));
             std::vector<int> tg(nt), tl(nt);
             std::vector<double> ts(nt);
@@ -868,10 +875,326 @@ bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts
     return BEC_OK;
 }
 
+namespace {
+
+// mu, energy per particle, norm and residual of an x-space state already on the device (FP64 kernels)
+bec_status plain_measures(bec_ctx *ctx, const GeomD &g, double2 *a, double2 *tmp, double2 *tmp2, bec_gs_report *rep)
+{
+    cudaStream_t s = ctx->stream;
+    double *sc = ctx->d_scal, *red = ctx->d_red;
+    const int cells = g.cells;
+    bec_status st;
+    plain_gs_xsums(a, g, sc + 8, red, s);
+    CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
+    if ((st = plain_fft(ctx, tmp, g, 1))) return st;
+    plain_scale(tmp, cells, 1.0 / cells, s);
+    plain_gs_ksum(tmp, g, sc + 12, red, s);
+    double h[8];
+    CKC(cudaMemcpyAsync(h, sc + 8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    const double ekin = h[4] * cells * g.dV, epot = h[0] * g.dV, eint = g.g11 * h[1] * g.dV, N = h[2] * g.dV;
+    const double mu = (ekin + epot + eint) / N;
+    rep->mu = mu;
+    rep->energy = (ekin + epot + 0.5 * eint) / N;
+    rep->N = N;
+    plain_mul_k2(tmp, tmp2, g, s);
+    if ((st = plain_fft(ctx, tmp2, g, 0))) return st;
+    plain_gs_residual(a, tmp2, g, mu, sc + 16, red, s);
+    double r2;
+    CKC(cudaMemcpyAsync(&r2, sc + 16, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    rep->residual = std::sqrt(r2 / h[2]);
+    CKL();
+    return BEC_OK;
+}
+
+struct GsClass {
+    ClassGeom geom{};
+    std::vector<int> groups;           // group of each local trajectory
+    std::vector<int> batch;            // its index in the caller's list
+    float2 *state = nullptr, *out = nullptr, *warm = nullptr;
+    int *d_tgroup = nullptr;
+    double *norm = nullptr;            // [2][n]
+    double *ekin = nullptr, *xsums = nullptr;
+};
+
+// Batched FP32 imaginary-time ground states for groups whose grids the register passes support.
+// psi_out (host states) may be NULL; coef_in (n x 64, host) seeds warm starts synthesised on the
+// device; coef_out (n x 64, host) receives the projections of the results on the correction basis.
+bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_opts *opts, double *const *psi_out,
+                      bec_gs_report *reports, const double *coef_in = nullptr, double *coef_out = nullptr)
+{
+    cudaStream_t s = ctx->stream;
+    const long long l0 = g_launches;
+    std::vector<GsClass> cls;
+    std::vector<int> cls_of(n), idx_in(n);
+    for (int i = 0; i < n; ++i) {
+        const bec_derived &d = ctx->groups[groups[i]].d;
+        int c = -1;
+        for (size_t k = 0; k < cls.size(); ++k)
+            if (cls[k].geom.nx == d.nvx && cls[k].geom.ny == d.nvy && cls[k].geom.nz == d.nvz) c = (int)k;
+        if (c < 0) {
+            GsClass gc;
+            gc.geom.nx = d.nvx; gc.geom.ny = d.nvy; gc.geom.nz = d.nvz;
+            gc.geom.lx = ilog2(d.nvx); gc.geom.ly = ilog2(d.nvy); gc.geom.lz = ilog2(d.nvz);
+            gc.geom.cells = d.cells;
+            cls.push_back(gc);
+            c = (int)cls.size() - 1;
+        }
+        cls_of[i] = c;
+        idx_in[i] = (int)cls[c].groups.size();
+        cls[c].groups.push_back(groups[i]);
+        cls[c].batch.push_back(i);
+    }
+    // offsets of per-group warm starts (back to back, in list order)
+    std::vector<size_t> warm_off(n + 1, 0);
+    for (int i = 0; i < n; ++i) warm_off[i + 1] = warm_off[i] + (size_t)ctx->groups[groups[i]].d.cells;
+    // per-group FP32 parameters for the whole context (indexed by group)
+    std::vector<GsParamsF> hp(ctx->groups.size());
+    for (size_t g = 0; g < ctx->groups.size(); ++g) {
+        const bec_derived &d = ctx->groups[g].d;
+        hp[g].N = d.N;
+        hp[g].parseval = (double)d.cells * d.dV;
+        hp[g].dt_steady = (float)d.dt_steady;
+        hp[g].mu = (float)d.mu;
+    }
+    std::vector<void *> tmp_allocs;
+    struct Free { std::vector<void *> &v; cudaStream_t s; ~Free() { cudaStreamSynchronize(s); for (void *p : v) cudaFree(p); } } fr{tmp_allocs, s};
+    auto talloc = [&](void **p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+        if (e == cudaSuccess) tmp_allocs.push_back(*p);
+        return e;
+    };
+    GsParamsF *d_gs = nullptr;
+    CKC(talloc((void **)&d_gs, sizeof(GsParamsF) * hp.size()));
+    CKC(cudaMemcpyAsync(d_gs, hp.data(), sizeof(GsParamsF) * hp.size(), cudaMemcpyHostToDevice, s));
+    // GroupParamsF of every group (the batched context has them already; the plain one does not)
+    GroupParamsF *d_gp = ctx->d_gparams;
+    if (!d_gp) {
+        std::vector<GroupParamsF> gfs(ctx->groups.size());
+        for (size_t g = 0; g < gfs.size(); ++g) gfs[g] = ctx->groups[g].gf;
+        CKC(talloc((void **)&d_gp, sizeof(GroupParamsF) * gfs.size()));
+        CKC(cudaMemcpyAsync(d_gp, gfs.data(), sizeof(GroupParamsF) * gfs.size(), cudaMemcpyHostToDevice, s));
+    }
+    for (auto &c : cls) {
+        const size_t nt = c.groups.size(), cells = c.geom.cells;
+        c.geom.n_traj = (int)nt;
+        CKC(talloc((void **)&c.state, sizeof(float2) * nt * cells));
+        CKC(talloc((void **)&c.out, sizeof(float2) * nt * cells));
+        CKC(talloc((void **)&c.d_tgroup, sizeof(int) * nt));
+        CKC(talloc((void **)&c.norm, sizeof(double) * 2 * nt));
+        CKC(talloc((void **)&c.ekin, sizeof(double) * nt));
+        CKC(talloc((void **)&c.xsums, sizeof(double) * 3 * nt));
+        CKC(cudaMemcpyAsync(c.d_tgroup, c.groups.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
+        CKC(cudaMemsetAsync(c.norm, 0, sizeof(double) * 2 * nt, s));
+        if (opts->warm_start) {
+            std::vector<float2> h(nt * cells);
+            for (size_t t = 0; t < nt; ++t)
+                for (size_t i = 0; i < cells; ++i) {
+                    const size_t src = (opts->warm_per_group ? warm_off[c.batch[t]] : 0) + i;
+                    h[t * cells + i] = make_float2((float)opts->warm_start[2 * src], (float)opts->warm_start[2 * src + 1]);
+                }
+            CKC(talloc((void **)&c.warm, sizeof(float2) * nt * cells));
+            CKC(cudaMemcpy(c.warm, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+        } else if (coef_in) {
+            const int nb = warmstart_basis_size();
+            std::vector<double> cc(nt * nb);
+            std::vector<bec_derived> dd(nt);
+            for (size_t t = 0; t < nt; ++t) {
+                dd[t] = ctx->groups[c.groups[t]].d;
+                for (int k = 0; k < nb; ++k) cc[t * nb + k] = coef_in[(size_t)c.batch[t] * nb + k];
+            }
+            CKC(talloc((void **)&c.warm, sizeof(float2) * nt * cells));
+            CKC(warmstart_synth(cc.data(), (int)nt, dd.data(), c.warm, s));
+        }
+    }
+    auto tw_for = [&](int nz, float2 **tw) { return get_tw32_full(ctx, nz, tw); };
+    bec_status st;
+    CKC(cudaEventRecord(ctx->ev0, s));
+    // start: x-space profile -> stored form; measure its norm, first half kick of step 0
+    for (auto &c : cls) {
+        float2 *tw;
+        if ((st = tw_for(c.geom.nz, &tw))) return st;
+        gs_init(c.state, c.geom, d_gp, d_gs, c.d_tgroup, c.warm, s);
+        gs_prep(c.state, c.geom, d_gp, d_gs, c.d_tgroup, s);
+        gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.0f, 0.5f, 1.0f / c.geom.cells, 1.0f, c.norm,
+                  nullptr, s);
+    }
+    CKL();
+    const int maxs = opts->max_steps > 0 ? opts->max_steps : 1;
+    const int check = opts->check_every > 0 ? opts->check_every : 1;
+    const bool mu_mode = opts->mode == BEC_GS_MU;
+    std::vector<std::vector<double>> mu_prev(cls.size()), conv_step(cls.size());
+    for (size_t k = 0; k < cls.size(); ++k) {
+        mu_prev[k].assign(cls[k].groups.size(), 0.0);
+        conv_step[k].assign(cls[k].groups.size(), -1.0);
+    }
+    int steps = 0;
+    bool converged_all = false;
+    // measures the boundary state after `steps` steps: writes out (renormalised x-space) and mu per trajectory
+    auto boundary = [&](bool final_pass, std::vector<std::vector<double>> *mus) -> bec_status {
+        const int b = steps & 1;            // buffer the closing pencil pass measures into
+        for (auto &c : cls) {
+            float2 *tw;
+            bec_status st2;
+            if ((st2 = tw_for(c.geom.nz, &tw))) return st2;
+            const int nt = c.geom.n_traj;
+            CKC(cudaMemsetAsync(c.ekin, 0, sizeof(double) * nt, s));
+            CKC(cudaMemsetAsync(c.xsums, 0, sizeof(double) * 3 * nt, s));
+            gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.0f, 1.0f / c.geom.cells,
+                      (float)(c.geom.nx * c.geom.ny), c.norm + (size_t)b * nt, c.ekin, s);
+            gs_output(c.state, c.geom, d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt, c.out, c.xsums,
+                      1.0f / (float)(c.geom.nx * c.geom.ny), s);
+            if (!final_pass)   // resume: first half kick of the next step, norm already measured
+                gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.0f, 0.5f, 1.0f / c.geom.cells, 1.0f,
+                          nullptr, nullptr, s);
+        }
+        CKL();
+        if (mus) {
+            for (size_t k = 0; k < cls.size(); ++k) {
+                auto &c = cls[k];
+                const int nt = c.geom.n_traj;
+                std::vector<double> nrm(nt), ek(nt), xs(3 * nt);
+                CKC(cudaMemcpyAsync(nrm.data(), c.norm + (size_t)b * nt, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+                CKC(cudaMemcpyAsync(ek.data(), c.ekin, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+                CKC(cudaMemcpyAsync(xs.data(), c.xsums, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, s));
+                CKC(cudaStreamSynchronize(s));
+                (*mus)[k].resize(nt);
+                for (int t = 0; t < nt; ++t) {
+                    const bec_derived &d = ctx->groups[c.groups[t]].d;
+                    const double s2 = d.N / (nrm[t] * (double)d.cells * d.dV);       // renormalisation squared
+                    const double e_kin = ek[t] * s2 * (double)d.cells * d.dV;
+                    const double N = xs[3 * t + 2] * d.dV;
+                    (*mus)[k][t] = (e_kin + xs[3 * t] * d.dV + d.g11 * xs[3 * t + 1] * d.dV) / N;
+                }
+            }
+        }
+        return BEC_OK;
+    };
+    while (steps < maxs) {
+        const int b = steps & 1;
+        for (auto &c : cls) {
+            const int nt = c.geom.n_traj;
+            gs_plane_step(c.state, c.geom, d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt,
+                          c.norm + (size_t)(b ^ 1) * nt, s);
+        }
+        CKL();
+        ++steps;
+        const bool last = steps == maxs;
+        if (mu_mode && (steps % check) == 0 && !last) {
+            std::vector<std::vector<double>> mus(cls.size());
+            if ((st = boundary(false, &mus))) return st;
+            bool all = true;
+            for (size_t k = 0; k < cls.size(); ++k)
+                for (size_t t = 0; t < mus[k].size(); ++t) {
+                    const double m = mus[k][t];
+                    if (!std::isfinite(m)) return fail(ctx, BEC_ERR_NUMERICAL, "ground state diverged");
+                    if (conv_step[k][t] < 0 && mu_prev[k][t] != 0.0 && std::fabs((m - mu_prev[k][t]) / m) < opts->tol)
+                        conv_step[k][t] = steps;
+                    mu_prev[k][t] = m;
+                    all = all && conv_step[k][t] >= 0;
+                }
+            if (all) { converged_all = true; break; }
+        } else if (!last) {
+            for (auto &c : cls) {
+                float2 *tw;
+                if ((st = tw_for(c.geom.nz, &tw))) return st;
+                const int nt = c.geom.n_traj;
+                gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.5f, 1.0f / c.geom.cells, 1.0f,
+                          c.norm + (size_t)((steps & 1)) * nt, nullptr, s);
+            }
+            CKL();
+        }
+    }
+    // after a check at which every trajectory converged, out already holds the renormalised boundary state
+    if (!converged_all && (st = boundary(true, nullptr))) return st;
+    CKC(cudaEventRecord(ctx->ev1, s));
+    CKC(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    // outputs, FP64 measures of each ground state on the device
+    size_t maxc = 0;
+    for (auto &c : cls) maxc = std::max(maxc, (size_t)c.geom.cells);
+    double2 *a64 = nullptr, *t1 = nullptr, *t2 = nullptr;
+    CKC(talloc((void **)&a64, sizeof(double2) * maxc));
+    CKC(talloc((void **)&t1, sizeof(double2) * maxc));
+    CKC(talloc((void **)&t2, sizeof(double2) * maxc));
+    for (int i = 0; i < n; ++i) {
+        GsClass &c = cls[cls_of[i]];
+        const size_t cells = c.geom.cells;
+        const float2 *src = c.out + (size_t)idx_in[i] * cells;
+        if (psi_out) {
+            std::vector<float2> h(cells);
+            CKC(cudaMemcpyAsync(h.data(), src, sizeof(float2) * cells, cudaMemcpyDeviceToHost, s));
+            CKC(cudaStreamSynchronize(s));
+            for (size_t k = 0; k < cells; ++k) { psi_out[i][2 * k] = h[k].x; psi_out[i][2 * k + 1] = h[k].y; }
+        }
+        if (reports) {
+            bec_gs_report &r = reports[i];
+            std::memset(&r, 0, sizeof(r));
+            const double cs = conv_step[cls_of[i]][idx_in[i]];
+            r.converged = mu_mode ? (cs >= 0 ? 1 : 0) : 0;
+            r.steps = (mu_mode && cs >= 0) ? (int)cs : steps;
+            r.seconds = ms * 1e-3;
+            gs_to_double(src, a64, cells, s);
+            if ((st = plain_measures(ctx, ctx->groups[groups[i]].gd, a64, t1, t2, &r))) return st;
+        }
+    }
+    if (coef_out) {
+        const int nb = warmstart_basis_size();
+        for (auto &c : cls) {
+            const size_t nt = c.groups.size();
+            std::vector<bec_derived> dd(nt);
+            for (size_t t = 0; t < nt; ++t) dd[t] = ctx->groups[c.groups[t]].d;
+            std::vector<double> cc(nt * nb);
+            CKC(warmstart_project(c.out, (int)nt, dd.data(), cc.data(), s));
+            for (size_t t = 0; t < nt; ++t)
+                for (int k = 0; k < nb; ++k) coef_out[(size_t)c.batch[t] * nb + k] = cc[t * nb + k];
+        }
+    }
+    ctx->last_launches = g_launches - l0;
+    ctx->last_ms = ms;
+    return BEC_OK;
+}
+
+} // namespace
+
+bec_status bec_ground_state_coeffs(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
+                                   const double *coef_in, double *coef_out, bec_gs_report *reports)
+{
+    if (!ctx || n < 1 || !groups || !opts) return BEC_ERR_INVALID_ARG;
+    if (ctx->path != BEC_PATH_FP32_BATCHED || opts->mode == BEC_GS_REFERENCE_E || opts->warm_start)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "coefficient ground states need the batched path, FIXED or MU rules");
+    const bec_derived &d0 = ctx->groups[groups[0]].d;
+    for (int i = 0; i < n; ++i) {
+        if (groups[i] < 0 || groups[i] >= (int)ctx->groups.size()) return fail(ctx, BEC_ERR_INVALID_ARG, "bad group");
+        const bec_derived &d = ctx->groups[groups[i]].d;
+        ClassGeom g{};
+        g.nx = d.nvx; g.ny = d.nvy; g.nz = d.nvz; g.n_traj = 4;
+        if (d.nvx != d0.nvx || d.nvy != d0.nvy || d.nvz != d0.nvz || !gs_batched_supported(g))
+            return fail(ctx, BEC_ERR_UNSUPPORTED_GRID, "coefficient ground states need one supported grid");
+    }
+    return gs_batched(ctx, n, groups, opts, nullptr, reports, coef_in, coef_out);
+}
+
+int32_t bec_warmstart_basis_size(void) { return warmstart_basis_size(); }
+
 bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
                                   double *const *psi_out, bec_gs_report *reports)
 {
-    if (!ctx || n < 0 || (n > 0 && (!groups || !psi_out))) return BEC_ERR_INVALID_ARG;
+    if (!ctx || n < 0 || (n > 0 && (!groups || !psi_out || !opts))) return BEC_ERR_INVALID_ARG;
+    for (int i = 0; i < n; ++i)
+        if (groups[i] < 0 || groups[i] >= (int)ctx->groups.size() || !psi_out[i])
+            return fail(ctx, BEC_ERR_INVALID_ARG, "bad group index or output pointer");
+    // the batched FP32 path: FIXED_STEPS or MU rules on grids the register passes cover
+    bool batched = ctx->path == BEC_PATH_FP32_BATCHED && opts->mode != BEC_GS_REFERENCE_E && n > 0;
+    for (int i = 0; batched && i < n; ++i) {
+        const bec_derived &d = ctx->groups[groups[i]].d;
+        ClassGeom g{};
+        g.nx = d.nvx; g.ny = d.nvy; g.nz = d.nvz; g.n_traj = 4;
+        if (!gs_batched_supported(g)) batched = false;
+    }
+    if (batched) return gs_batched(ctx, n, groups, opts, psi_out, reports);
     for (int i = 0; i < n; ++i) {
         bec_status st = bec_ground_state(ctx, groups[i], opts, psi_out[i], reports ? &reports[i] : nullptr);
         if (st) return st;
@@ -973,6 +1296,31 @@ bec_status bec_pulse(bec_ctx *ctx, double theta, double phi)
     double2 m[4];
     rotation(theta, phi, m);
     return apply_pulse(ctx, m);
+}
+
+bec_status bec_pulse_finite(bec_ctx *ctx, double rabi_hz, double duration_s, double phi)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!(duration_s > 0) || !std::isfinite(rabi_hz) || !std::isfinite(phi))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad pulse parameters");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    const double dt = ctx->groups[0].p.dt_evo;
+    for (auto &g : ctx->groups)
+        if (g.p.dt_evo != dt) return fail(ctx, BEC_ERR_INVALID_ARG, "finite pulses need one dt_evo for all groups");
+    const long long n = std::max(1LL, (long long)std::llround(duration_s / dt));
+    const double half = 0.5 * 2.0 * M_PI * rabi_hz * (duration_s / (double)n);   // Omega dt_sub / 2
+    double2 m[4];
+    rotation(half, phi, m);
+    const long long l0 = g_launches;
+    for (long long k = 0; k < n; ++k) {
+        if ((st = apply_pulse(ctx, m))) return st;
+        if ((st = do_evolve(ctx, 1))) return st;
+        if ((st = apply_pulse(ctx, m))) return st;
+    }
+    ctx->last_launches = g_launches - l0;
+    CKC(cudaStreamSynchronize(ctx->stream));
+    return BEC_OK;
 }
 
 bec_status bec_start_evolution(bec_ctx *ctx)
@@ -1102,17 +1450,17 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
     } else {
         bool obs_due = false;
         for (int i = 1; i <= n; ++i) {
-            // z pass: finishes step i-1 (observing its end state if due), starts step i
-            const double2 *m2 = nullptr;
-            if (i - 1 == sch->pi_pulse_step) m2 = pi_m;
-            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, obs_due, m2))) return st;
-            ctx->pending = true;
             if (obs_due) {
+                // observe the boundary after step i-1 with a pass that ends that step
+                if ((st = batched_resolve(ctx, true))) return st;
                 if ((st = batched_reduce_obs(ctx))) return st;
-                // the moments belong to the boundary before this step: evo_steps = i - 1
                 if ((st = take_sample())) return st;
                 obs_due = false;
             }
+            // a pi pulse scheduled after step i-1 rides on this step's pencil pass (after any sample)
+            if (i - 1 == sch->pi_pulse_step && (st = apply_pulse(ctx, pi_m))) return st;
+            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
+            ctx->pending = true;
             if ((st = batched_ppass_all(ctx))) return st;
             ctx->step++;
             ctx->evo_steps++;

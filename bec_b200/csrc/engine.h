@@ -109,6 +109,35 @@ void obs_reduce(const double *obs_partial, int n_traj, int tiles, int nz, const 
 void group_reduce(const double *traj_tot, const int *group_first, const int *group_count, int n_groups,
                   double *out, cudaStream_t s);
 
+// gs_passes.cu: batched FP32 imaginary-time ground states (one trajectory per group)
+struct GsParamsF {
+    double N;                 // target norm
+    double parseval;          // cells * dV: N' = parseval * sum |psi_k|^2
+    float dt_steady;          // natural units
+    float mu;                 // Thomas-Fermi chemical potential (start profile)
+};
+bool gs_batched_supported(const ClassGeom &c);
+void gs_init(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
+             const float2 *warm, cudaStream_t s);
+void gs_prep(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
+             cudaStream_t s);
+void gs_plane_step(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
+                   const double *norm_in, double *norm_clear, cudaStream_t s);
+// FFT_xy of the stored state times in_scale * sqrt(N / N'): x-space rows to out, sums (n V, n^2, n) to xsums
+void gs_output(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
+               const double *norm_in, float2 *out, double *xsums, float in_scale, cudaStream_t s);
+// kick exp(-dt frac1 k^2/2) * scale [measure] then exp(-dt frac2 k^2/2) * out_scale
+void gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
+               const float2 *tw_full, float frac1, float frac2, float scale, float out_scale, double *norm,
+               double *ekin, cudaStream_t s);
+
+void gs_to_double(const float2 *in, double2 *out, size_t n, cudaStream_t s);
+
+// warmstart.cu: the 64-term correction over Thomas-Fermi (one grid per call)
+int warmstart_basis_size();
+cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, double *coef_out, cudaStream_t s);
+cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, float2 *psi_out, cudaStream_t s);
+
 // launch counter (kernels this library enqueued since the counter was reset)
 extern thread_local long long g_launches;
 
@@ -117,7 +146,10 @@ bool fp32_fast_plane_supported(const ClassGeom &c);
 bool fp32_fast_pencil_supported(const ClassGeom &c);
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
                      uint32_t step, cudaStream_t s);
-// tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times the output scale;
-// m: optional pulse matrix (row-major, 4 entries) or NULL
+// tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times out_scale;
+// m: optional pulse matrix (row-major, 4 entries) or NULL; obs: when not NULL the pass
+// ends a step and writes per-z partial moments [traj][tile][z][4] (tiles = fp32_fast_pencil_tiles)
 void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
-                      const float2 *tw_full, float frac, float scale, const float2 *m, cudaStream_t s);
+                      const float2 *tw_full, float frac, float scale, const float2 *m, double *obs,
+                      float out_scale, cudaStream_t s);
+int fp32_fast_pencil_tiles(const ClassGeom &c);

@@ -118,11 +118,14 @@ struct PencilArgs {
     float2 m[4];         // pulse matrix, row-major
 };
 
-template <int NZ>
+// OBS: the pass ends a step (no plane pass follows) and also writes, per z, the
+// FP64 sums over the tile's 16 pencils of |a|^2, |b|^2 and conj(a) b of the
+// z-transformed boundary state: obs[((traj * tiles + tile) * NZ + z) * 4 + k].
+template <int NZ, bool OBS>
 __global__ void __launch_bounds__(NZ) k_pencil(float4 *__restrict__ state, int nx, int lx, int ny, int cells,
                                                int tiles, const GroupParamsF *__restrict__ gp,
                                                const int *__restrict__ tgroup, const float2 *__restrict__ tw_g,
-                                               PencilArgs pa)
+                                               PencilArgs pa, double *__restrict__ obs, float inv_out_scale)
 {
     constexpr int R = 16, G = NZ / 16;
     extern __shared__ float4 dyn[];
@@ -214,22 +217,48 @@ __global__ void __launch_bounds__(NZ) k_pencil(float4 *__restrict__ state, int n
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[(p * G + j) * R + (k1 ^ (p & 7))];
     dft<R, false>(x);
+    if constexpr (OBS) {
+        // the output is out_scale * FFT_z(boundary state); undo the scale for the moments
+        __syncthreads();                                        // stage-3 reads of buf done
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const float4 v = x[m];
+            const float ax = v.x * inv_out_scale, ay = v.y * inv_out_scale;
+            const float bx = v.z * inv_out_scale, by = v.w * inv_out_scale;
+            const int z = j + G * m;
+            buf[p * NZ + (z ^ (p & 7))] = make_float4(ax * ax + ay * ay, bx * bx + by * by, ax * bx + ay * by,
+                                                      ax * by - ay * bx);
+        }
+        __syncthreads();
+        const int tile = blockIdx.x - traj * tiles;
+        for (int z = t; z < NZ; z += blockDim.x) {
+            KSum s0, s1, s2, s3;
+#pragma unroll
+            for (int q2 = 0; q2 < 16; ++q2) {
+                const float4 u = buf[q2 * NZ + (z ^ (q2 & 7))];
+                s0.add(u.x); s1.add(u.y); s2.add(u.z); s3.add(u.w);
+            }
+            double *o = obs + (((size_t)traj * tiles + tile) * NZ + z) * 4;
+            o[0] = s0.value(); o[1] = s1.value(); o[2] = s2.value(); o[3] = s3.value();
+        }
+    }
 #pragma unroll
     for (int m = 0; m < R; ++m) g[(size_t)(j + G * m) * plane] = x[m];
 }
 
-template <int NZ>
+template <int NZ, bool OBS>
 void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const float2 *tw,
-                   const PencilArgs &pa, cudaStream_t s)
+                   const PencilArgs &pa, double *obs, float inv_out_scale, cudaStream_t s)
 {
     const int tiles = c.nx * c.ny / 16;
     const size_t smem = sizeof(float4) * 16 * NZ + sizeof(float2) * (2 * NZ + 16);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_pencil<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_pencil<NZ, OBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_pencil<NZ><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, tgroup, tw, pa);
+    k_pencil<NZ, OBS><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, tgroup, tw,
+                                                         pa, obs, inv_out_scale);
     g_launches++;
 }
 
@@ -276,7 +305,8 @@ void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, 
 }
 
 void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
-                      const float2 *tw_full, float frac, float scale, const float2 *m, cudaStream_t s)
+                      const float2 *tw_full, float frac, float scale, const float2 *m, double *obs,
+                      float out_scale, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
     PencilArgs pa{};
@@ -285,10 +315,22 @@ void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp,
     pa.has_m = m ? 1 : 0;
     if (m)
         for (int i = 0; i < 4; ++i) pa.m[i] = m[i];
+    const float inv = 1.0f / out_scale;
     switch (c.nz) {
-    case 64: launch_pencil<64>(state, c, gp, tgroup, tw_full, pa, s); break;
-    case 128: launch_pencil<128>(state, c, gp, tgroup, tw_full, pa, s); break;
-    case 256: launch_pencil<256>(state, c, gp, tgroup, tw_full, pa, s); break;
+    case 64:
+        if (obs) launch_pencil<64, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
+        else launch_pencil<64, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        break;
+    case 128:
+        if (obs) launch_pencil<128, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
+        else launch_pencil<128, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        break;
+    case 256:
+        if (obs) launch_pencil<256, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
+        else launch_pencil<256, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        break;
     default: break;
     }
 }
+
+int fp32_fast_pencil_tiles(const ClassGeom &c) { return c.nx * c.ny / 16; }

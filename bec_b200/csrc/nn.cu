@@ -1,0 +1,524 @@
+// nn.cu -- the warm-start network: a small MLP trained and evaluated on the GPU.
+//
+// No counterpart in the reference. The network maps an ensemble's parameters
+// to the coefficients of a correction to the Thomas-Fermi profile; its output
+// only seeds the imaginary-time ground-state loop (bec_ground_state_batch),
+// which remains the judge of convergence.
+//
+// Layers are Y = act(X W^T + b) (W is [out x in], row-major, as a linear layer),
+// tanh on hidden layers, identity on the last. GEMMs run on the tensor cores with
+// BF16 operands and FP32 accumulation (mma.sync m16n8k16); master weights, Adam
+// moments, activations' pre-images and gradients are FP32.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "engine.h"
+
+namespace {
+
+constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+
+// C[M x N] = A[M x K] * B[N x K]^T (+ bias[N]); A, B BF16 row-major; C FP32.
+// M, N multiples of 64; K multiple of 32. 128 threads: 2 x 2 warps of 32 x 32.
+__global__ void __launch_bounds__(128) k_gemm_bt(const __nv_bfloat16 *__restrict__ A,
+                                                 const __nv_bfloat16 *__restrict__ B, float *__restrict__ C,
+                                                 const float *__restrict__ bias, int M, int N, int K)
+{
+    __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PAD];
+    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PAD];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int gid = lane >> 2, tig = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+
+    for (int k0 = 0; k0 < K; k0 += TK) {
+        // 64 x 32 bf16 tile = 256 chunks of 8 elements (16 bytes); 2 per thread and operand
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int chunk = t + c * 128;
+            const int row = chunk >> 2, col = (chunk & 3) * 8;
+            *reinterpret_cast<uint4 *>(&As[row][col]) =
+                *reinterpret_cast<const uint4 *>(A + (size_t)(m0 + row) * K + k0 + col);
+            *reinterpret_cast<uint4 *>(&Bs[row][col]) =
+                *reinterpret_cast<const uint4 *>(B + (size_t)(n0 + row) * K + k0 + col);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 16) {
+            uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + gid;
+                af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + tig * 2]);
+                af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + tig * 2]);
+                af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + tig * 2 + 8]);
+                af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + tig * 2 + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int n = wn + j * 8 + gid;
+                bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[n][kk + tig * 2]);
+                bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[n][kk + tig * 2 + 8]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    asm volatile(
+                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+                        : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]),
+                          "r"(bfr[j][1]));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = m0 + wm + i * 16 + gid;
+            const int c = n0 + wn + j * 8 + tig * 2;
+            const float b0 = bias ? bias[c] : 0.0f, b1 = bias ? bias[c + 1] : 0.0f;
+            C[(size_t)r * N + c] = acc[i][j][0] + b0;
+            C[(size_t)r * N + c + 1] = acc[i][j][1] + b1;
+            C[(size_t)(r + 8) * N + c] = acc[i][j][2] + b0;
+            C[(size_t)(r + 8) * N + c + 1] = acc[i][j][3] + b1;
+        }
+}
+
+// y = tanh(z) (or z on the output layer) as BF16 for the next GEMM, FP32 copy kept
+__global__ void k_act(const float *z, float *y, __nv_bfloat16 *ybf, size_t n, int linear)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = linear ? z[i] : tanhf(z[i]);
+        y[i] = v;
+        if (ybf) ybf[i] = __float2bfloat16(v);
+    }
+}
+
+// dZ = dY * (1 - y^2) (tanh) or dY (linear)
+__global__ void k_act_back(const float *dy, const float *y, float *dz, size_t n, int linear)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dz[i] = linear ? dy[i] : dy[i] * (1.0f - y[i] * y[i]);
+}
+
+// out[c][r] = bf16(in[r][c]) for an R x Cn FP32 matrix (also plain casts with transpose = 0)
+__global__ void k_cast_t(const float *in, __nv_bfloat16 *out, int R, int Cn, int transpose)
+{
+    const size_t n = (size_t)R * Cn;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / Cn), c = (int)(i - (size_t)r * Cn);
+        out[transpose ? (size_t)c * R + r : i] = __float2bfloat16(in[i]);
+    }
+}
+
+// db[c] = sum_r dz[r][c]
+__global__ void k_colsum(const float *dz, float *db, int R, int Cn)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Cn) return;
+    float s = 0.0f;
+    for (int r = 0; r < R; ++r) s += dz[(size_t)r * Cn + c];
+    db[c] = s;
+}
+
+// dY = 2 (y - t) / (B * out) over the first `valid` rows (padding rows get 0); loss partials
+__global__ void k_mse(const float *y, const float *tgt, float *dy, int rows, int valid, int cols, float *loss)
+{
+    const size_t n = (size_t)rows * cols;
+    float l = 0.0f;
+    const float s = 2.0f / ((float)valid * cols);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols);
+        const float d = (r < valid) ? y[i] - tgt[i] : 0.0f;
+        dy[i] = s * d;
+        l += d * d;
+    }
+    for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l / ((float)valid * cols));
+}
+
+__global__ void k_adam(float *w, float *m, float *v, const float *g, size_t n, float lr, float b1, float b2, float eps,
+                       float c1, float c2)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// gather rows idx[r] of src (n_src x cols) into dst (rows x cols), zero rows past `valid`
+__global__ void k_gather(const float *src, const int *idx, float *dst, int rows, int valid, int cols)
+{
+    const size_t n = (size_t)rows * cols;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols), c = (int)(i - (size_t)r * cols);
+        dst[i] = (r < valid) ? src[(size_t)idx[r] * cols + c] : 0.0f;
+    }
+}
+
+inline int grid_for(size_t n) { size_t b = (n + 255) / 256; return (int)(b > 4096 ? 4096 : (b < 1 ? 1 : b)); }
+
+} // namespace
+
+struct bec_mlp {
+    std::vector<int> w;              // widths (padded): w[0] = padded inputs
+    std::vector<int> w_real;         // caller's widths
+    int L = 0;                       // weight layers
+    std::vector<size_t> woff, boff;  // offsets into the parameter vector
+    size_t n_params = 0;
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // FP32 params, grads, Adam moments
+    __nv_bfloat16 *pbf = nullptr;    // BF16 weights [out x in]
+    __nv_bfloat16 *wt = nullptr;     // scratch for W^T
+    int cap = 0;                     // batch capacity of the activation buffers
+    std::vector<float *> z, y;       // per layer: pre-activation, activation (FP32) [cap x w]
+    std::vector<__nv_bfloat16 *> xbf; // per layer input in BF16 [cap x w]
+    float *dy = nullptr, *dz = nullptr, *loss = nullptr;
+    __nv_bfloat16 *tA = nullptr, *tB = nullptr;
+    int *idx = nullptr;
+    float *xin = nullptr, *tgt = nullptr;
+    long long adam_t = 0;
+    cudaStream_t s = nullptr;
+    std::string err;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+bec_status mlp_alloc(bec_mlp *m, void **p, size_t bytes)
+{
+    if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) { cudaGetLastError(); return BEC_ERR_OUT_OF_MEMORY; }
+    m->allocs.push_back(*p);
+    return BEC_OK;
+}
+
+int round_up(int v, int q) { return (v + q - 1) / q * q; }
+
+bec_status mlp_reserve(bec_mlp *m, int batch)
+{
+    if (batch <= m->cap) return BEC_OK;
+    const int cap = round_up(batch, 64);
+    int maxw = 0;
+    for (int v : m->w) maxw = std::max(maxw, v);
+    m->z.assign(m->L + 1, nullptr);
+    m->y.assign(m->L + 1, nullptr);
+    m->xbf.assign(m->L + 1, nullptr);
+    bec_status st;
+    for (int l = 0; l <= m->L; ++l) {
+        if ((st = mlp_alloc(m, (void **)&m->z[l], sizeof(float) * cap * m->w[l]))) return st;
+        if ((st = mlp_alloc(m, (void **)&m->y[l], sizeof(float) * cap * m->w[l]))) return st;
+        if ((st = mlp_alloc(m, (void **)&m->xbf[l], sizeof(__nv_bfloat16) * cap * m->w[l]))) return st;
+    }
+    if ((st = mlp_alloc(m, (void **)&m->dy, sizeof(float) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->dz, sizeof(float) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->tA, sizeof(__nv_bfloat16) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->tB, sizeof(__nv_bfloat16) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->tgt, sizeof(float) * cap * m->w[m->L]))) return st;
+    m->cap = cap;
+    return BEC_OK;
+}
+
+// forward on the first `rows` (multiple of 64) rows of y[0] (FP32 inputs, padded)
+void mlp_forward_dev(bec_mlp *m, int rows)
+{
+    cudaStream_t s = m->s;
+    k_cast_t<<<grid_for((size_t)rows * m->w[0]), 256, 0, s>>>(m->y[0], m->xbf[0], rows, m->w[0], 0);
+    for (int l = 0; l < m->L; ++l) {
+        const int in = m->w[l], out = m->w[l + 1];
+        dim3 grid(out / TN, rows / TM);
+        k_gemm_bt<<<grid, 128, 0, s>>>(m->xbf[l], m->pbf + m->woff[l], m->z[l + 1], m->p + m->boff[l], rows, out, in);
+        const int linear = (l == m->L - 1);
+        k_act<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->z[l + 1], m->y[l + 1], m->xbf[l + 1],
+                                                           (size_t)rows * out, linear);
+        g_launches += 2;
+    }
+    g_launches++;
+}
+
+// gradients of the MSE loss into m->g, after mlp_forward_dev; targets in m->tgt
+void mlp_backward_dev(bec_mlp *m, int rows, int valid)
+{
+    cudaStream_t s = m->s;
+    const int outw = m->w[m->L];
+    cudaMemsetAsync(m->loss, 0, sizeof(float), s);
+    k_mse<<<grid_for((size_t)rows * outw), 256, 0, s>>>(m->y[m->L], m->tgt, m->dy, rows, valid, outw, m->loss);
+    g_launches++;
+    for (int l = m->L - 1; l >= 0; --l) {
+        const int in = m->w[l], out = m->w[l + 1];
+        const int linear = (l == m->L - 1);
+        k_act_back<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dy, m->y[l + 1], m->dz, (size_t)rows * out, linear);
+        k_colsum<<<(out + 127) / 128, 128, 0, s>>>(m->dz, m->g + m->boff[l], rows, out);
+        // dW [out x in] = dZ^T [out x rows] * (X^T [in x rows])^T
+        k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 1);
+        k_cast_t<<<grid_for((size_t)rows * in), 256, 0, s>>>(m->y[l], m->tB, rows, in, 1);
+        {
+            dim3 grid(in / TN, out / TM);
+            k_gemm_bt<<<grid, 128, 0, s>>>(m->tA, m->tB, m->g + m->woff[l], nullptr, out, in, rows);
+        }
+        g_launches += 5;
+        if (l > 0) {
+            // dX [rows x in] = dZ [rows x out] * W [out x in] = dZ * (W^T [in x out])^T
+            k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 0);
+            k_cast_t<<<grid_for((size_t)out * in), 256, 0, s>>>(m->p + m->woff[l], m->wt, out, in, 1);
+            dim3 grid(in / TN, rows / TM);
+            k_gemm_bt<<<grid, 128, 0, s>>>(m->tA, m->wt, m->dy, nullptr, rows, in, out);
+            g_launches += 3;
+        }
+    }
+}
+
+void mlp_sync_bf16(bec_mlp *m)
+{
+    for (int l = 0; l < m->L; ++l) {
+        k_cast_t<<<grid_for((size_t)m->w[l] * m->w[l + 1]), 256, 0, m->s>>>(m->p + m->woff[l], m->pbf + m->woff[l],
+                                                                             m->w[l + 1], m->w[l], 0);
+        g_launches++;
+    }
+}
+
+// host x (batch x real_in) -> device y[0] (rows x padded_in)
+bec_status upload_inputs(bec_mlp *m, const float *x, int batch, int rows)
+{
+    std::vector<float> h((size_t)rows * m->w[0], 0.0f);
+    for (int r = 0; r < batch; ++r)
+        for (int c = 0; c < m->w_real[0]; ++c) h[(size_t)r * m->w[0] + c] = x[(size_t)r * m->w_real[0] + c];
+    if (cudaMemcpyAsync(m->y[0], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, m->s) != cudaSuccess)
+        return BEC_ERR_CUDA;
+    return cudaStreamSynchronize(m->s) == cudaSuccess ? BEC_OK : BEC_ERR_CUDA;
+}
+
+} // namespace
+
+extern "C" {
+
+bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed, bec_mlp **out)
+{
+    if (!out) return BEC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!widths || n_layers < 1 || n_layers > 16) return BEC_ERR_INVALID_ARG;
+    for (int l = 0; l <= n_layers; ++l)
+        if (widths[l] < 1 || widths[l] > 4096) return BEC_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return BEC_ERR_NO_DEVICE; }
+    bec_mlp *m = new bec_mlp();
+    m->L = n_layers;
+    m->w_real.assign(widths, widths + n_layers + 1);
+    m->w.resize(n_layers + 1);
+    for (int l = 0; l <= n_layers; ++l) m->w[l] = round_up(widths[l], 64);   // GEMM tiles are 64 wide
+    for (int l = 0; l < n_layers; ++l) {
+        m->woff.push_back(m->n_params);
+        m->n_params += (size_t)m->w[l] * m->w[l + 1];
+        m->boff.push_back(m->n_params);
+        m->n_params += (size_t)m->w[l + 1];
+    }
+    auto bail = [&](bec_status st) { bec_mlp_destroy(m); return st; };
+    bec_status st;
+    if (cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) != cudaSuccess) return bail(BEC_ERR_CUDA);
+    if ((st = mlp_alloc(m, (void **)&m->p, sizeof(float) * m->n_params))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->g, sizeof(float) * m->n_params))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->m, sizeof(float) * m->n_params))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->v, sizeof(float) * m->n_params))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->pbf, sizeof(__nv_bfloat16) * m->n_params))) return bail(st);
+    int maxw = 0;
+    for (int v : m->w) maxw = std::max(maxw, v);
+    if ((st = mlp_alloc(m, (void **)&m->wt, sizeof(__nv_bfloat16) * maxw * maxw))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->loss, sizeof(float)))) return bail(st);
+    // Glorot-uniform weights on the real block, zero padding and biases
+    std::vector<float> h(m->n_params, 0.0f);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < n_layers; ++l) {
+        const float a = std::sqrt(6.0f / (float)(widths[l] + widths[l + 1]));
+        std::uniform_real_distribution<float> U(-a, a);
+        for (int o = 0; o < widths[l + 1]; ++o)
+            for (int i = 0; i < widths[l]; ++i) h[m->woff[l] + (size_t)o * m->w[l] + i] = U(rng);
+    }
+    cudaMemcpy(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
+    cudaMemset(m->m, 0, sizeof(float) * m->n_params);
+    cudaMemset(m->v, 0, sizeof(float) * m->n_params);
+    mlp_sync_bf16(m);
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);
+    *out = m;
+    return BEC_OK;
+}
+
+void bec_mlp_destroy(bec_mlp *m)
+{
+    if (!m) return;
+    if (m->s) cudaStreamSynchronize(m->s);
+    for (void *p : m->allocs) cudaFree(p);
+    if (m->s) cudaStreamDestroy(m->s);
+    delete m;
+}
+
+int64_t bec_mlp_param_count(const bec_mlp *m)
+{
+    if (!m) return 0;
+    int64_t n = 0;
+    for (int l = 0; l < m->L; ++l) n += (int64_t)m->w_real[l] * m->w_real[l + 1] + m->w_real[l + 1];
+    return n;
+}
+
+// host layout: for each layer W [out x in] row-major then b [out] (caller's widths)
+bec_status bec_mlp_get_params(bec_mlp *m, float *params)
+{
+    if (!m || !params) return BEC_ERR_INVALID_ARG;
+    std::vector<float> h(m->n_params);
+    if (cudaMemcpy(h.data(), m->p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return BEC_ERR_CUDA;
+    size_t k = 0;
+    for (int l = 0; l < m->L; ++l) {
+        for (int o = 0; o < m->w_real[l + 1]; ++o)
+            for (int i = 0; i < m->w_real[l]; ++i) params[k++] = h[m->woff[l] + (size_t)o * m->w[l] + i];
+        for (int o = 0; o < m->w_real[l + 1]; ++o) params[k++] = h[m->boff[l] + o];
+    }
+    return BEC_OK;
+}
+
+bec_status bec_mlp_set_params(bec_mlp *m, const float *params)
+{
+    if (!m || !params) return BEC_ERR_INVALID_ARG;
+    std::vector<float> h(m->n_params, 0.0f);
+    size_t k = 0;
+    for (int l = 0; l < m->L; ++l) {
+        for (int o = 0; o < m->w_real[l + 1]; ++o)
+            for (int i = 0; i < m->w_real[l]; ++i) h[m->woff[l] + (size_t)o * m->w[l] + i] = params[k++];
+        for (int o = 0; o < m->w_real[l + 1]; ++o) h[m->boff[l] + o] = params[k++];
+    }
+    if (cudaMemcpy(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return BEC_ERR_CUDA;
+    mlp_sync_bf16(m);
+    return cudaStreamSynchronize(m->s) == cudaSuccess ? BEC_OK : BEC_ERR_CUDA;
+}
+
+bec_status bec_mlp_forward(bec_mlp *m, const float *x, int32_t batch, float *y)
+{
+    if (!m || !x || !y || batch < 1) return BEC_ERR_INVALID_ARG;
+    const int rows = round_up(batch, 64);
+    bec_status st;
+    if ((st = mlp_reserve(m, rows))) return st;
+    if ((st = upload_inputs(m, x, batch, rows))) return st;
+    mlp_forward_dev(m, rows);
+    const int ow = m->w[m->L];
+    std::vector<float> h((size_t)rows * ow);
+    if (cudaMemcpyAsync(h.data(), m->y[m->L], sizeof(float) * h.size(), cudaMemcpyDeviceToHost, m->s) != cudaSuccess)
+        return BEC_ERR_CUDA;
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    for (int r = 0; r < batch; ++r)
+        for (int c = 0; c < m->w_real[m->L]; ++c) y[(size_t)r * m->w_real[m->L] + c] = h[(size_t)r * ow + c];
+    return BEC_OK;
+}
+
+// Loss and gradients of mean((y - target)^2) over the batch (host params layout).
+bec_status bec_mlp_gradients(bec_mlp *m, const float *x, const float *target, int32_t batch, float *loss,
+                             float *grads)
+{
+    if (!m || !x || !target || batch < 1) return BEC_ERR_INVALID_ARG;
+    const int rows = round_up(batch, 64);
+    bec_status st;
+    if ((st = mlp_reserve(m, rows))) return st;
+    if ((st = upload_inputs(m, x, batch, rows))) return st;
+    const int ow = m->w[m->L];
+    std::vector<float> t((size_t)rows * ow, 0.0f);
+    for (int r = 0; r < batch; ++r)
+        for (int c = 0; c < m->w_real[m->L]; ++c) t[(size_t)r * ow + c] = target[(size_t)r * m->w_real[m->L] + c];
+    cudaMemcpyAsync(m->tgt, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice, m->s);
+    mlp_forward_dev(m, rows);
+    mlp_backward_dev(m, rows, batch);
+    float l = 0.f;
+    cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->s);
+    std::vector<float> h(m->n_params);
+    cudaMemcpyAsync(h.data(), m->g, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, m->s);
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    if (loss) *loss = l;
+    if (grads) {
+        size_t k = 0;
+        for (int li = 0; li < m->L; ++li) {
+            for (int o = 0; o < m->w_real[li + 1]; ++o)
+                for (int i = 0; i < m->w_real[li]; ++i) grads[k++] = h[m->woff[li] + (size_t)o * m->w[li] + i];
+            for (int o = 0; o < m->w_real[li + 1]; ++o) grads[k++] = h[m->boff[li] + o];
+        }
+    }
+    return BEC_OK;
+}
+
+// Adam on minibatches drawn (seeded) from n samples; loss_history[s] = loss of step s.
+bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_t n, int32_t batch, int32_t steps,
+                         float lr, uint64_t seed, float *loss_history)
+{
+    if (!m || !x || !target || n < 1 || batch < 1 || steps < 0) return BEC_ERR_INVALID_ARG;
+    const int rows = round_up(batch, 64);
+    bec_status st;
+    if ((st = mlp_reserve(m, rows))) return st;
+    const int in_r = m->w_real[0], out_r = m->w_real[m->L], inw = m->w[0], ow = m->w[m->L];
+    float *dx = nullptr, *dt = nullptr;
+    int *didx = nullptr;
+    std::vector<void *> loc;
+    auto lalloc = [&](void **p, size_t b) {
+        cudaError_t e = cudaMalloc(p, b);
+        if (e == cudaSuccess) loc.push_back(*p);
+        return e;
+    };
+    struct F { std::vector<void *> &v; cudaStream_t s; ~F() { cudaStreamSynchronize(s); for (void *p : v) cudaFree(p); } } f{loc, m->s};
+    if (lalloc((void **)&dx, sizeof(float) * (size_t)n * inw) || lalloc((void **)&dt, sizeof(float) * (size_t)n * ow) ||
+        lalloc((void **)&didx, sizeof(int) * rows))
+        return BEC_ERR_OUT_OF_MEMORY;
+    {
+        std::vector<float> hx((size_t)n * inw, 0.0f), ht((size_t)n * ow, 0.0f);
+        for (int r = 0; r < n; ++r) {
+            for (int c = 0; c < in_r; ++c) hx[(size_t)r * inw + c] = x[(size_t)r * in_r + c];
+            for (int c = 0; c < out_r; ++c) ht[(size_t)r * ow + c] = target[(size_t)r * out_r + c];
+        }
+        cudaMemcpy(dx, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(dt, ht.data(), sizeof(float) * ht.size(), cudaMemcpyHostToDevice);
+    }
+    std::mt19937_64 rng(seed);
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    int pos = n;
+    std::vector<int> hidx(rows, 0);
+    const int valid = std::min(batch, n);
+    std::vector<float> hist(steps, 0.0f);
+    for (int s = 0; s < steps; ++s) {
+        for (int r = 0; r < valid; ++r) {
+            if (pos >= n) { std::shuffle(order.begin(), order.end(), rng); pos = 0; }
+            hidx[r] = order[pos++];
+        }
+        cudaMemcpyAsync(didx, hidx.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, m->s);
+        k_gather<<<grid_for((size_t)rows * inw), 256, 0, m->s>>>(dx, didx, m->y[0], rows, valid, inw);
+        k_gather<<<grid_for((size_t)rows * ow), 256, 0, m->s>>>(dt, didx, m->tgt, rows, valid, ow);
+        mlp_forward_dev(m, rows);
+        mlp_backward_dev(m, rows, valid);
+        ++m->adam_t;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.0f - std::pow(b1, (float)m->adam_t), c2 = 1.0f - std::pow(b2, (float)m->adam_t);
+        k_adam<<<grid_for(m->n_params), 256, 0, m->s>>>(m->p, m->m, m->v, m->g, m->n_params, lr, b1, b2, 1e-8f, c1, c2);
+        mlp_sync_bf16(m);
+        cudaMemcpyAsync(&hist[s], m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->s);
+        g_launches += 3;
+        // the host copy of the batch indices must not be overwritten before its transfer
+        cudaStreamSynchronize(m->s);
+    }
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    if (loss_history)
+        for (int s = 0; s < steps; ++s) loss_history[s] = hist[s];
+    return cudaGetLastError() == cudaSuccess ? BEC_OK : BEC_ERR_CUDA;
+}
+
+} // extern "C"

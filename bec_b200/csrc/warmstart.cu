@@ -1,0 +1,257 @@
+// warmstart.cu -- the 64-term correction over Thomas-Fermi used by the warm start.
+//
+// No counterpart in the reference. A ground state psi of an ensemble is written
+// in Thomas-Fermi-scaled coordinates X = x/R, Y = y/R, Zs = z/(lambda R) with
+// R = sqrt(2 mu_TF) (the grid spans +-1.2 in each of them for every parameter
+// set, wigner.cpp:153-160), amplitude unit A = sqrt(mu_TF / g11):
+//     psi / A = f_TF(u) + sum_{i<16, j<4} c_ij B_ij,   f_TF = sqrt(max(1 - u, 0)),
+//     B_ij = exp(-((r - r_i) / w_i)^2) P_j(2 cos^2(theta) - 1),
+// u = X^2 + Y^2 + Zs^2 = r^2, cos^2(theta) = Zs^2 / u, P_j the Legendre
+// polynomials. Four broad radial bumps cover the interior (kinetic-energy
+// correction) and twelve narrow ones the condensate edge, where the ground
+// state departs most from Thomas-Fermi. The projection solves the normal
+// equations of this basis on the grid; the synthesis evaluates the expansion.
+#include <cmath>
+#include <vector>
+
+#include "engine.h"
+
+namespace {
+
+constexpr int kRad = 16, kAng = 4, kBasis = kRad * kAng;
+
+__device__ __constant__ float c_rc[kRad];   // radial centres
+__device__ __constant__ float c_rw[kRad];   // radial widths
+
+struct WsGeom {
+    int nx, ny, nz, lx, ly, cells;
+    float dxs, dys, dzs;        // grid steps in scaled units
+};
+
+__device__ __forceinline__ void basis_at(int i, const WsGeom &g, float *b, float &ftf)
+{
+    const int x = i & (g.nx - 1), y = (i >> g.lx) & (g.ny - 1), z = i >> (g.lx + g.ly);
+    const float X = -1.2f + g.dxs * x;
+    const float Y = (g.ny > 1) ? -1.2f + g.dys * y : 0.0f;
+    const float Z = -1.2f + g.dzs * z;
+    const float u = X * X + Y * Y + Z * Z;
+    const float r = sqrtf(u);
+    const float c2 = (u > 0.0f) ? Z * Z / u : 0.0f;
+    const float q = 2.0f * c2 - 1.0f;
+    const float p[kAng] = {1.0f, q, 0.5f * (3.0f * q * q - 1.0f), 0.5f * q * (5.0f * q * q - 3.0f)};
+    ftf = sqrtf(fmaxf(1.0f - u, 0.0f));
+#pragma unroll
+    for (int a = 0; a < kRad; ++a) {
+        const float d = (r - c_rc[a]) / c_rw[a];
+        const float e = __expf(-d * d);
+#pragma unroll
+        for (int j = 0; j < kAng; ++j) b[a * kAng + j] = e * p[j];
+    }
+}
+
+// rhs[t][k] = sum_cells B_k (|psi_t| / A_t - f_TF); gram[k][l] = sum_cells B_k B_l (if gram != NULL)
+__global__ void k_ws_project(const float2 *psi, int n_traj, WsGeom g, const float *amp, double *rhs, double *gram)
+{
+    const int t = blockIdx.y;
+    __shared__ double acc[kBasis];
+    for (int k = threadIdx.x; k < kBasis; k += blockDim.x) acc[k] = 0.0;
+    __syncthreads();
+    float loc[kBasis];
+#pragma unroll
+    for (int k = 0; k < kBasis; ++k) loc[k] = 0.0f;
+    const float inv_a = 1.0f / amp[t];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.cells; i += gridDim.x * blockDim.x) {
+        float b[kBasis], ftf;
+        basis_at(i, g, b, ftf);
+        const float2 v = psi[(size_t)t * g.cells + i];
+        const float d = sqrtf(v.x * v.x + v.y * v.y) * inv_a - ftf;
+#pragma unroll
+        for (int k = 0; k < kBasis; ++k) loc[k] += b[k] * d;
+    }
+#pragma unroll
+    for (int k = 0; k < kBasis; ++k) {
+        float v = loc[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&acc[k], (double)v);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kBasis; k += blockDim.x) atomicAdd(rhs + (size_t)t * kBasis + k, acc[k]);
+}
+
+// gram[k][l] = sum_cells B_k B_l: 256 threads, each owns 16 of the 64 x 64 entries; the basis
+// rows of 32 cells at a time are staged in shared memory.
+__global__ void __launch_bounds__(256) k_ws_gram(WsGeom g, double *gram)
+{
+    __shared__ float rows[32][kBasis];
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+    const int t = threadIdx.x;
+    const int k = t >> 2, l0 = (t & 3) * 16;   // row k, columns l0 .. l0 + 15
+    for (int base = blockIdx.x * 32; base < g.cells; base += gridDim.x * 32) {
+        if (t < 32) {
+            float b[kBasis], ftf;
+            const int i = base + t;
+            if (i < g.cells) {
+                basis_at(i, g, b, ftf);
+#pragma unroll
+                for (int q = 0; q < kBasis; ++q) rows[t][q] = b[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < kBasis; ++q) rows[t][q] = 0.0f;
+            }
+        }
+        __syncthreads();
+        float part[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) part[e] = 0.0f;
+        for (int c = 0; c < 32; ++c) {
+            const float bk = rows[c][k];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) part[e] += bk * rows[c][l0 + e];
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[e] += part[e];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) atomicAdd(gram + k * kBasis + l0 + e, acc[e]);
+}
+
+// psi_t = A_t max(f_TF + sum c_k B_k, 0) (real, x-space)
+__global__ void k_ws_synth(float2 *psi, int n_traj, WsGeom g, const float *amp, const float *coef)
+{
+    const int t = blockIdx.y;
+    __shared__ float c[kBasis];
+    for (int k = threadIdx.x; k < kBasis; k += blockDim.x) c[k] = coef[(size_t)t * kBasis + k];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.cells; i += gridDim.x * blockDim.x) {
+        float b[kBasis], ftf;
+        basis_at(i, g, b, ftf);
+        float f = ftf;
+#pragma unroll
+        for (int k = 0; k < kBasis; ++k) f += c[k] * b[k];
+        psi[(size_t)t * g.cells + i] = make_float2(amp[t] * fmaxf(f, 0.0f), 0.0f);
+    }
+}
+
+bool g_consts_set = false;
+
+cudaError_t set_consts()
+{
+    if (g_consts_set) return cudaSuccess;
+    float rc[kRad], rw[kRad];
+    const float broad[4] = {0.0f, 0.3f, 0.55f, 0.75f};
+    for (int a = 0; a < 4; ++a) { rc[a] = broad[a]; rw[a] = 0.22f; }
+    for (int a = 4; a < kRad; ++a) { rc[a] = 0.80f + 0.045f * (a - 4); rw[a] = 0.06f; }
+    cudaError_t e = cudaMemcpyToSymbol(c_rc, rc, sizeof(rc));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rw, rw, sizeof(rw));
+    if (e == cudaSuccess) g_consts_set = true;
+    return e;
+}
+
+WsGeom geom_of(const bec_derived &d)
+{
+    WsGeom g{};
+    g.nx = d.nvx; g.ny = d.nvy; g.nz = d.nvz;
+    int lx = 0, ly = 0;
+    while ((1 << lx) < d.nvx) ++lx;
+    while ((1 << ly) < d.nvy) ++ly;
+    g.lx = lx; g.ly = ly;
+    g.cells = d.cells;
+    g.dxs = 2.4f / (float)(d.nvx - 1);
+    g.dys = d.nvy > 1 ? 2.4f / (float)(d.nvy - 1) : 0.0f;
+    g.dzs = 2.4f / (float)(d.nvz - 1);
+    return g;
+}
+
+// Cholesky solve of the SPD system G c = r (G upper triangle given), in place on copies
+bool chol_solve(std::vector<double> G, const double *r, double *c, int n)
+{
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < i; ++j) G[i * n + j] = G[j * n + i];
+    double ridge = 1e-10 * G[0];
+    for (int i = 0; i < n; ++i) G[i * n + i] += ridge;
+    for (int j = 0; j < n; ++j) {
+        double s = G[j * n + j];
+        for (int k = 0; k < j; ++k) s -= G[j * n + k] * G[j * n + k];
+        if (s <= 0) return false;
+        const double d = std::sqrt(s);
+        G[j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double t = G[i * n + j];
+            for (int k = 0; k < j; ++k) t -= G[i * n + k] * G[j * n + k];
+            G[i * n + j] = t / d;
+        }
+    }
+    std::vector<double> y(n);
+    for (int i = 0; i < n; ++i) {
+        double t = r[i];
+        for (int k = 0; k < i; ++k) t -= G[i * n + k] * y[k];
+        y[i] = t / G[i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double t = y[i];
+        for (int k = i + 1; k < n; ++k) t -= G[k * n + i] * c[k];
+        c[i] = t / G[i * n + i];
+    }
+    return true;
+}
+
+} // namespace
+
+int warmstart_basis_size() { return kBasis; }
+
+// psi: n x cells x-space states (float2, device) of ensembles with derived parameters d[t]; coef: n x 64 (host)
+cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, double *coef_out, cudaStream_t s)
+{
+    cudaError_t e = set_consts();
+    if (e) return e;
+    const WsGeom g = geom_of(d[0]);
+    std::vector<float> amp(n);
+    for (int t = 0; t < n; ++t) amp[t] = (float)std::sqrt(d[t].mu / d[t].g11);
+    float *damp = nullptr;
+    double *rhs = nullptr, *gram = nullptr;
+    if ((e = cudaMalloc(&damp, sizeof(float) * n))) return e;
+    if ((e = cudaMalloc(&rhs, sizeof(double) * n * kBasis))) { cudaFree(damp); return e; }
+    if ((e = cudaMalloc(&gram, sizeof(double) * kBasis * kBasis))) { cudaFree(damp); cudaFree(rhs); return e; }
+    cudaMemcpyAsync(damp, amp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(rhs, 0, sizeof(double) * n * kBasis, s);
+    cudaMemsetAsync(gram, 0, sizeof(double) * kBasis * kBasis, s);
+    dim3 grid(64, n);
+    k_ws_project<<<grid, 256, 0, s>>>(psi, n, g, damp, rhs, nullptr);
+    k_ws_gram<<<148, 256, 0, s>>>(g, gram);
+    g_launches += 2;
+    std::vector<double> hr((size_t)n * kBasis), hg(kBasis * kBasis);
+    cudaMemcpyAsync(hr.data(), rhs, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hg.data(), gram, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    cudaFree(damp); cudaFree(rhs); cudaFree(gram);
+    if (e) return e;
+    for (int t = 0; t < n; ++t)
+        if (!chol_solve(hg, hr.data() + (size_t)t * kBasis, coef_out + (size_t)t * kBasis, kBasis))
+            return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// coef: n x 64 (host); psi_out: n x cells float2 (device)
+cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, float2 *psi_out, cudaStream_t s)
+{
+    cudaError_t e = set_consts();
+    if (e) return e;
+    const WsGeom g = geom_of(d[0]);
+    std::vector<float> amp(n), c((size_t)n * kBasis);
+    for (int t = 0; t < n; ++t) amp[t] = (float)std::sqrt(d[t].mu / d[t].g11);
+    for (size_t k = 0; k < c.size(); ++k) c[k] = (float)coef[k];
+    float *damp = nullptr, *dc = nullptr;
+    if ((e = cudaMalloc(&damp, sizeof(float) * n))) return e;
+    if ((e = cudaMalloc(&dc, sizeof(float) * c.size()))) { cudaFree(damp); return e; }
+    cudaMemcpyAsync(damp, amp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dc, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice, s);
+    dim3 grid(64, n);
+    k_ws_synth<<<grid, 256, 0, s>>>(psi_out, n, g, damp, dc);
+    g_launches++;
+    e = cudaStreamSynchronize(s);
+    cudaFree(damp); cudaFree(dc);
+    return e ? e : cudaGetLastError();
+}

@@ -54,6 +54,20 @@ SIGNATURES = {
                                     _P(C.c_int32)]),
     "bec_moments_device_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,
                                              C.c_void_p]),
+    "bec_ground_state_coeffs": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32), _P(BecGsOpts), _dp, _dp,
+                                          _P(BecGsReport)]),
+    "bec_warmstart_basis_size": (C.c_int32, []),
+    "bec_pulse_finite": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    "bec_mlp_create": (C.c_int, [_P(C.c_int32), C.c_int32, C.c_uint64, _P(C.c_void_p)]),
+    "bec_mlp_destroy": (None, [C.c_void_p]),
+    "bec_mlp_param_count": (C.c_int64, [C.c_void_p]),
+    "bec_mlp_get_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "bec_mlp_set_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "bec_mlp_forward": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int32, _P(C.c_float)]),
+    "bec_mlp_gradients": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), C.c_int32, _P(C.c_float),
+                                    _P(C.c_float)]),
+    "bec_mlp_train": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), C.c_int32, C.c_int32, C.c_int32,
+                                C.c_float, C.c_uint64, _P(C.c_float)]),
 }
 
 
@@ -192,6 +206,11 @@ class Engine:
     def pulse(self, theta, phi=0.0):
         self._check(lib().bec_pulse(self._h, float(theta), float(phi)), "bec_pulse")
 
+    def pulse_finite(self, rabi_hz, duration_s, phi=0.0):
+        """Rabi pulse of finite duration (coupling on during round(duration/dt) split steps)."""
+        self._check(lib().bec_pulse_finite(self._h, float(rabi_hz), float(duration_s), float(phi)),
+                    "bec_pulse_finite")
+
     # ---- observables
     def moments(self):
         ms = (BecMoments * self.n_groups)()
@@ -265,4 +284,69 @@ class Engine:
         self._check(lib().bec_set_state(self._h, group, traj, _dptr(ab.view(np.float64))), "bec_set_state")
 
 
-__all__ = ["Engine", "BecError", "derive", "lib", "BEC_PATH_FP32_BATCHED", "BEC_PATH_FP64_PLAIN"]
+def _fptr(a):
+    return a.ctypes.data_as(_P(C.c_float))
+
+
+class MLP:
+    """The warm-start network (bec_mlp_*): tanh MLP, BF16 tensor-core GEMMs, FP32 accumulation."""
+
+    def __init__(self, widths, seed=0):
+        self.widths = [int(w) for w in widths]
+        arr = (C.c_int32 * len(self.widths))(*self.widths)
+        h = C.c_void_p()
+        st = lib().bec_mlp_create(arr, len(self.widths) - 1, seed, C.byref(h))
+        if st:
+            raise BecError(st, "bec_mlp_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bec_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, st, what):
+        if st:
+            raise BecError(st, what)
+
+    @property
+    def n_params(self):
+        return int(lib().bec_mlp_param_count(self._h))
+
+    def get_params(self):
+        p = np.zeros(self.n_params, dtype=np.float32)
+        self._check(lib().bec_mlp_get_params(self._h, _fptr(p)), "bec_mlp_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(lib().bec_mlp_set_params(self._h, _fptr(p)), "bec_mlp_set_params")
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], self.widths[-1]), dtype=np.float32)
+        self._check(lib().bec_mlp_forward(self._h, _fptr(x), x.shape[0], _fptr(y)), "bec_mlp_forward")
+        return y
+
+    def gradients(self, x, target):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_float()
+        self._check(lib().bec_mlp_gradients(self._h, _fptr(x), _fptr(t), x.shape[0], C.byref(loss), _fptr(g)),
+                    "bec_mlp_gradients")
+        return float(loss.value), g
+
+    def train(self, x, target, steps, batch=256, lr=1e-3, seed=0):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        hist = np.zeros(max(steps, 1), dtype=np.float32)
+        self._check(lib().bec_mlp_train(self._h, _fptr(x), _fptr(t), x.shape[0], batch, steps, lr, seed,
+                                        _fptr(hist)), "bec_mlp_train")
+        return hist[:steps]
+
+
+__all__ = ["Engine", "MLP", "BecError", "derive", "lib", "BEC_PATH_FP32_BATCHED", "BEC_PATH_FP64_PLAIN"]

@@ -41,7 +41,7 @@ WORKLOAD = "uneven-ensembles-1024"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="bec", choices=["bec", "reference"])
     ap.add_argument("--n-traj", type=int, default=N_TRAJ)
@@ -135,38 +135,48 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(groups, seconds, steps_per_rep=1):
-    """Times the oracle (FP64 CPU restatement) on a bounded sample of the workload,
-    one trajectory per thread on all host cores. Returns (traj-steps/s, cores, sample)."""
-    from concurrent.futures import ThreadPoolExecutor
-    from oracle import oracle as O
-    cores = os.cpu_count() or 1
-    n = max(3, min(len(groups), 2 * cores))
-    sample = groups[:n]
-    ens = []
-    for p in sample:
-        e = O.OracleEnsemble(p)
-        e.init(thomas_fermi(O.derive(p)))
-        ens.append(e)
+class OracleSample:
+    """A bounded sample of the workload on the CPU oracle (FP64 restatement of the
+    reference's split step), one trajectory per thread on all host cores."""
 
-    def work(e):
-        e.evolve(steps_per_rep, 1)
+    def __init__(self, groups):
+        from concurrent.futures import ThreadPoolExecutor
+        from oracle import oracle as O
+        self.cores = os.cpu_count() or 1
+        self.sample = groups[:max(3, min(len(groups), 2 * self.cores))]
+        self.ens = []
+        for p in self.sample:
+            e = O.OracleEnsemble(p)
+            e.init(thomas_fermi(O.derive(p)))
+            self.ens.append(e)
+        self.pool = ThreadPoolExecutor(max_workers=self.cores)
 
-    with ThreadPoolExecutor(max_workers=cores) as ex:
+    def step(self):
+        """One split step of every sampled trajectory; returns the wall time."""
         t0 = time.perf_counter()
-        list(ex.map(work, ens))
-        t1 = time.perf_counter()
-        reps = max(1, int(seconds / max(t1 - t0, 1e-3)))
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            list(ex.map(work, ens))
-        el = time.perf_counter() - t0
-    v = n * steps_per_rep * reps / el
-    grids = {}
-    for p in sample:
-        k = f"{p.nvx}x{p.nvy}x{p.nvz}"
-        grids[k] = grids.get(k, 0) + 1
-    return v, cores, f"{n} trajectories of the workload mix {grids}, {reps * steps_per_rep} steps, {el:.1f} s"
+        list(self.pool.map(lambda e: e.evolve(1, 1), self.ens))
+        return time.perf_counter() - t0
+
+    def describe(self, steps, seconds):
+        grids = {}
+        for p in self.sample:
+            k = f"{p.nvx}x{p.nvy}x{p.nvz}"
+            grids[k] = grids.get(k, 0) + 1
+        return f"{len(self.sample)} trajectories of the workload mix {grids}, {steps} steps, {seconds:.1f} s"
+
+    def close(self):
+        self.pool.shutdown()
+
+
+def cpu_baseline(groups, seconds):
+    """Oracle throughput on the sample for about `seconds`: (traj-steps/s, cores, sample)."""
+    s = OracleSample(groups)
+    s.step()
+    reps = max(1, int(seconds / max(s.step(), 1e-3)))
+    el = sum(s.step() for _ in range(reps))
+    v = len(s.sample) * reps / el
+    s.close()
+    return v, s.cores, s.describe(reps, el)
 
 
 def run_reference(args, ws, rank):
@@ -174,21 +184,22 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     groups = config2(n_traj=args.n_traj, seed=2, grids=grid_mix(args))
-    vals = []
-    sample = ""
-    cores = os.cpu_count() or 1
-    per = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    s = OracleSample(groups)
     for _ in range(args.warmup):
-        cpu_baseline(groups, 0.2)
-    for _ in range(args.steps):
-        v, cores, sample = cpu_baseline(groups, per)
-        vals.append(v)
-    v = statistics.mean(vals)
+        s.step()
+    # each bench step is one oracle step of the sample, capped so the run stays within minutes
+    steps = min(args.steps, max(3, int(args.cpu_seconds * 6 / max(s.step(), 1e-3))))
+    el = sum(s.step() for _ in range(steps))
+    v = len(s.sample) * steps / el
+    cores, sample = s.cores, s.describe(steps, el)
+    s.close()
     line = {
         "impl": "reference", "metric": "wigner_traj_steps_per_s", "value": v, "unit": "traj-steps/s",
-        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "n_gpus": ws, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_traj": args.n_traj, "grids": "8x8x64/16x16x128/32x32x256",
+        "config": {"workload": WORKLOAD if not args.grids else f"{args.n_traj}x{args.grids}", "n_traj": args.n_traj,
+                   "grids": args.grids or "8x8x64/16x16x128/32x32x256 uniform",
+                   "step": "one split step of every trajectory of a bounded sample of the workload",
                    "implementation": "CPU FP64 restatement of the reference's split step (oracle port)"},
         "cpu_baseline": {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

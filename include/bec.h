@@ -118,7 +118,7 @@ typedef struct bec_gs_opts {
     int32_t mode;            /* BEC_GS_* */
     int32_t max_steps;       /* step cap (the exact count for FIXED_STEPS) */
     int32_t check_every;     /* steps between convergence checks (MU mode) */
-    int32_t reserved;
+    int32_t warm_per_group;  /* bec_ground_state_batch: 1 = warm_start holds one start per listed group, back to back */
     double tol;              /* relative tolerance for MU mode (REFERENCE_E uses 1e-6) */
     const double *warm_start;/* optional x-space start (interleaved complex, cells); NULL = Thomas-Fermi */
 } bec_gs_opts;
@@ -197,6 +197,18 @@ bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups
                                   const bec_gs_opts *opts, double *const *psi_out,
                                   bec_gs_report *reports);
 
+/* Ground states of n groups that share one grid, run batched in FP32 on the device
+ * (FIXED_STEPS or MU rules, batched path only), exchanging only coefficients of the
+ * 64-term correction over Thomas-Fermi with the host (bec_warmstart_basis_size):
+ *   coef_in  (n x 64, may be NULL): warm starts psi = A max(f_TF + sum c_k B_k, 0),
+ *            synthesised on the device (NULL = Thomas-Fermi);
+ *   coef_out (n x 64, may be NULL): least-squares projection of each result;
+ *   reports  (n, may be NULL): steps, convergence, mu, energy, residual (FP64 on the device).
+ * The basis and scaling are documented in bec_b200/csrc/warmstart.cu. */
+bec_status bec_ground_state_coeffs(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
+                                   const double *coef_in, double *coef_out, bec_gs_report *reports);
+int32_t bec_warmstart_basis_size(void);
+
 /* ---- evolution -------------------------------------------------------- */
 
 /* initializeEnsembles (wigner_kernel.cu:295-317) for one group:
@@ -215,6 +227,15 @@ bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps);
  * theta = pi/2, phi = 0 is applyHalfPiPulse (wigner_kernel.cu:320-329);
  * theta = pi, phi = 0 is applyPiPulse (:332-341). */
 bec_status bec_pulse(bec_ctx *ctx, double theta, double phi);
+
+/* A Rabi pulse of finite duration (the report's coupled equations, report.tex:305-330,
+ * which the reference only approximates by instantaneous rotations): the state
+ * evolves for round(duration / dt_evo) split steps with the coupling
+ * (Omega / 2)(e^{-i phi} |1><2| + h.c.) on, Omega = 2 pi rabi_hz, the detuning
+ * staying in the nonlinear step as in the reference. Each step is Strang-split
+ * as R(Omega dt / 2) . step . R(Omega dt / 2) with R the rotation of bec_pulse.
+ * Every group must share dt_evo. */
+bec_status bec_pulse_finite(bec_ctx *ctx, double rabi_hz, double duration_s, double phi);
 
 /* The reference's initEvolution (wigner.cu:202-227) after bec_init_group for every
  * group: the equilibration steps (t = 0; t <= t_equilib; t += dt_evo), then the
@@ -273,6 +294,32 @@ int64_t bec_last_launch_count(const bec_ctx *ctx);
  * steps (wigner.cpp:365-369). */
 bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes, int32_t *dims,
                              int64_t *traj, double *ms, int32_t *n_classes);
+
+/* ---- warm-start network ------------------------------------------------ */
+
+/*
+ * A multilayer perceptron Y = act(X W^T + b) per layer (tanh on hidden layers,
+ * identity on the last), trained and evaluated on the GPU with BF16
+ * tensor-core GEMMs accumulating in FP32. No counterpart in the reference: it
+ * predicts the coefficients of a correction to the Thomas-Fermi profile that
+ * seeds bec_ground_state_batch (warm_start), which stays the judge.
+ * widths has n_layers + 1 entries (inputs, hidden..., outputs). Host parameter
+ * layout: for each layer W [out x in] row-major, then b [out].
+ */
+typedef struct bec_mlp bec_mlp;
+bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed, bec_mlp **out);
+void bec_mlp_destroy(bec_mlp *m);
+int64_t bec_mlp_param_count(const bec_mlp *m);
+bec_status bec_mlp_get_params(bec_mlp *m, float *params);
+bec_status bec_mlp_set_params(bec_mlp *m, const float *params);
+/* x: batch x inputs, y: batch x outputs (host, FP32) */
+bec_status bec_mlp_forward(bec_mlp *m, const float *x, int32_t batch, float *y);
+/* loss = mean over the batch and outputs of (y - target)^2 and its gradient (host layout) */
+bec_status bec_mlp_gradients(bec_mlp *m, const float *x, const float *target, int32_t batch, float *loss,
+                             float *grads);
+/* Adam (beta 0.9, 0.999) on seeded minibatches of n samples; loss_history[step] (may be NULL) */
+bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_t n, int32_t batch, int32_t steps,
+                         float lr, uint64_t seed, float *loss_history);
 
 /* ---- moments without device allocation -------------------------------- */
 

@@ -1,0 +1,86 @@
+"""The warm-start MLP: the FP64 oracle against finite differences (CPU), and the
+GPU forward/backward kernels (BF16 tensor-core GEMMs, FP32 accumulation)
+against the oracle (GPU, called through the C ABI).
+
+Tolerances: the GPU rounds GEMM operands to bfloat16 exactly as the oracle's
+bf16 mode does, so the remaining differences are FP32 accumulation order and
+tanh in FP32: relative 2e-3 on gradients and outputs against the bf16-mode
+oracle, 3e-2 against plain FP64."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+
+WIDTHS = [6, 256, 256, 256, 64]
+
+
+def _data(n=200, seed=0, widths=WIDTHS):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1, 1, (n, widths[0]))
+    t = np.tanh(x @ rng.standard_normal((widths[0], widths[-1]))) * 0.5
+    return x.astype(np.float32), t.astype(np.float32)
+
+
+def _params(widths, seed=1):
+    rng = np.random.default_rng(seed)
+    Ws = [rng.uniform(-1, 1, (o, i)) * np.sqrt(6.0 / (i + o)) for i, o in zip(widths[:-1], widths[1:])]
+    bs = [rng.standard_normal(o) * 0.05 for o in widths[1:]]
+    return M.pack(Ws, bs).astype(np.float32)
+
+
+def test_bf16_rounding():
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 2 ** -9, -3.14159, 0.0, 1.0 + 3 * 2 ** -8], dtype=np.float32)
+    r = M.to_bf16(v)
+    assert r[0] == 1.0
+    assert r[1] == 1.0                 # halfway between 1 and 1 + 2^-7: ties to the even mantissa
+    assert r[2] == 1.0
+    assert r[5] == 1.0 + 2 ** -6       # halfway between 1 + 2^-7 and 1 + 2^-6: ties to even
+    assert abs(r[3] + 3.140625) < 1e-12
+    assert r[4] == 0.0
+
+
+def test_oracle_gradients_match_finite_differences():
+    widths = [3, 8, 8, 4]
+    x, t = _data(7, seed=3, widths=widths)
+    p = _params(widths).astype(np.float64)
+    _, g = M.loss_and_grads(p, widths, x, t)
+    rng = np.random.default_rng(0)
+    for k in rng.choice(p.size, 25, replace=False):
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        num = (M.loss_and_grads(p + e, widths, x, t)[0] - M.loss_and_grads(p - e, widths, x, t)[0]) / 2e-6
+        assert num == pytest.approx(g[k], rel=1e-5, abs=1e-9)
+
+
+@pytest.mark.gpu
+def test_gpu_forward_and_gradients_match_oracle():
+    from bec_b200.engine import MLP
+    x, t = _data(200)
+    p = _params(WIDTHS)
+    net = MLP(WIDTHS, seed=0)
+    net.set_params(p)
+    np.testing.assert_array_equal(net.get_params(), p)
+    y = net.forward(x)
+    y_o = M.forward(p, WIDTHS, x, bf16=True)[-1]
+    assert np.abs(y - y_o).max() < 2e-3 * np.abs(y_o).max()
+    loss, g = net.gradients(x, t)
+    loss_o, g_o = M.loss_and_grads(p, WIDTHS, x, t, bf16=True)
+    assert loss == pytest.approx(loss_o, rel=2e-3)
+    assert np.linalg.norm(g - g_o) < 2e-3 * np.linalg.norm(g_o)
+    _, g64 = M.loss_and_grads(p, WIDTHS, x, t, bf16=False)
+    assert np.linalg.norm(g - g64) < 3e-2 * np.linalg.norm(g64)
+    from parity_util import record
+    record("mlp_grad", rel_err_bf16=np.linalg.norm(g - g_o) / np.linalg.norm(g_o),
+           rel_err_fp64=np.linalg.norm(g - g64) / np.linalg.norm(g64))
+
+
+@pytest.mark.gpu
+def test_gpu_training_reduces_loss():
+    from bec_b200.engine import MLP
+    x, t = _data(1024, seed=5)
+    net = MLP(WIDTHS, seed=3)
+    hist = net.train(x, t, steps=400, batch=128, lr=1e-3, seed=1)
+    assert np.isfinite(hist).all()
+    assert hist[-20:].mean() < 0.1 * hist[:5].mean()
+    loss, _ = net.gradients(x, t)
+    assert loss < 0.1 * hist[:5].mean()
