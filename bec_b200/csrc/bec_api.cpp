@@ -1407,6 +1407,55 @@ bec_status bec_axial_now(bec_ctx *ctx, int32_t group, double *out)
     return group_axial_host(ctx, group, out);
 }
 
+bec_status bec_render_projections(bec_ctx *ctx, int32_t group, float *xy_a, float *xy_b, float *zy_a, float *zy_b,
+                                  float *levels_xy, float *levels_zy)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (group < 0 || group >= (int)ctx->groups.size() || !xy_a || !xy_b || !zy_a || !zy_b)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad render arguments");
+    if (ctx->path != BEC_PATH_FP32_BATCHED) return fail(ctx, BEC_ERR_UNIMPLEMENTED, "rendering needs the batched path");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    GroupRec &gr = ctx->groups[group];
+    ClassRec &c = ctx->classes[gr.cls];
+    cudaStream_t s = ctx->stream;
+    if ((st = batched_resolve(ctx, false))) return st;
+    const int nxy = c.geom.nx * c.geom.ny, nyz = c.geom.ny * c.geom.nz;
+    float *lev = nullptr;
+    float4 *rgba = nullptr;
+    CKC(cudaMalloc(&lev, sizeof(float) * 2 * (nxy + nyz)));
+    if (cudaMalloc(&rgba, sizeof(float4) * 2 * (nxy + nyz)) != cudaSuccess) {
+        cudaFree(lev);
+        return fail(ctx, BEC_ERR_OUT_OF_MEMORY, "render buffers");
+    }
+    struct G { float *l; float4 *r; cudaStream_t s; ~G() { cudaStreamSynchronize(s); cudaFree(l); cudaFree(r); } } guard{lev, rgba, s};
+    float *lxa = lev, *lxb = lev + nxy, *lza = lev + 2 * nxy, *lzb = lza + nyz;
+    CKC(cudaMemsetAsync(lev, 0, sizeof(float) * 2 * (nxy + nyz), s));
+    ClassGeom one = c.geom;
+    one.n_traj = 1;
+    float2 *tx, *ty;
+    if ((st = get_tw32(ctx, one.nx, &tx)) || (st = get_tw32(ctx, one.ny, &ty))) return st;
+    const float sub = (float)(gr.d.V / (2.0 * gr.d.dV));
+    for (int t = 0; t < gr.p.ne; ++t) {
+        CKC(cudaMemcpyAsync(ctx->scratch4, c.state + (size_t)(gr.local_first + t) * c.geom.cells,
+                            sizeof(float4) * c.geom.cells, cudaMemcpyDeviceToDevice, s));
+        fp32_unprep(ctx->scratch4, one, tx, ty, s);
+        render_project(ctx->scratch4, one, 1.0f / (float)nxy, sub, lxa, lxb, lza, lzb, s);
+    }
+    const double scale = 3.0 * gr.d.N * gr.p.ne / ((double)gr.d.cells * gr.d.dV);    // wigner.cu:418
+    render_colour(lxa, 2 * nxy, (float)(scale * c.geom.nz), rgba, s);
+    render_colour(lza, 2 * nyz, (float)(scale * c.geom.nx), rgba + 2 * nxy, s);
+    CKL();
+    CKC(cudaMemcpyAsync(xy_a, rgba, sizeof(float4) * nxy, cudaMemcpyDeviceToHost, s));
+    CKC(cudaMemcpyAsync(xy_b, rgba + nxy, sizeof(float4) * nxy, cudaMemcpyDeviceToHost, s));
+    CKC(cudaMemcpyAsync(zy_a, rgba + 2 * nxy, sizeof(float4) * nyz, cudaMemcpyDeviceToHost, s));
+    CKC(cudaMemcpyAsync(zy_b, rgba + 2 * nxy + nyz, sizeof(float4) * nyz, cudaMemcpyDeviceToHost, s));
+    if (levels_xy) CKC(cudaMemcpyAsync(levels_xy, lxa, sizeof(float) * 2 * nxy, cudaMemcpyDeviceToHost, s));
+    if (levels_zy) CKC(cudaMemcpyAsync(levels_zy, lza, sizeof(float) * 2 * nyz, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    return BEC_OK;
+}
+
 bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, double *axial)
 {
     if (!ctx) return BEC_ERR_INVALID_ARG;

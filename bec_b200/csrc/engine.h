@@ -138,6 +138,11 @@ int warmstart_basis_size();
 cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, double *coef_out, cudaStream_t s);
 cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, float2 *psi_out, cudaStream_t s);
 
+// render.cu: projections after the reference's second pi/2 and the colour ramp
+void render_project(const float4 *x, const ClassGeom &c, float in_scale, float sub, float *xy_a, float *xy_b,
+                    float *zy_a, float *zy_b, cudaStream_t s);
+void render_colour(const float *level, int n, float max_level, float4 *rgba, cudaStream_t s);
+
 // launch counter (kernels this library enqueued since the counter was reset)
 extern thread_local long long g_launches;
 

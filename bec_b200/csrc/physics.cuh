@@ -37,6 +37,31 @@ __device__ __forceinline__ void normals4_fast(uint32_t k0, uint32_t k1, uint32_t
     box_muller_fast(r.z, r.w, out[2], out[3]);
 }
 
+// (cos t, sin t): Taylor series in t^2 for |t| <= 0.5 (truncation < 1.2e-11, below
+// FP32 rounding), sincosf beyond.
+__device__ __forceinline__ float2 cis_small(float t)
+{
+    if (fabsf(t) <= 0.5f) {
+        const float u = t * t;
+        const float s = t * (1.f - u * (1.f / 6.f) * (1.f - u * (1.f / 20.f) * (1.f - u * (1.f / 42.f) *
+                                                                                    (1.f - u * (1.f / 72.f)))));
+        const float c = 1.f - u * 0.5f * (1.f - u * (1.f / 12.f) * (1.f - u * (1.f / 30.f) *
+                                                                   (1.f - u * (1.f / 56.f) * (1.f - u * (1.f / 90.f)))));
+        return make_float2(c, s);
+    }
+    float s, c;
+    sincosf(t, &s, &c);
+    return make_float2(c, s);
+}
+
+// exp(x): Taylor series for |x| <= 1/64 (truncation < 1e-11), expf beyond.
+__device__ __forceinline__ float exp_small(float x)
+{
+    if (fabsf(x) <= 0.015625f)
+        return 1.f + x * (1.f + x * 0.5f * (1.f + x * (1.f / 3.f) * (1.f + x * 0.25f * (1.f + x * 0.2f))));
+    return expf(x);
+}
+
 // One cell: v = (a, b) at the start of the substep, V the trap potential.
 __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupParamsF &P)
 {
@@ -50,12 +75,10 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupP
         const float pa_im = V + P.g11 * na + P.g12 * nb;
         const float pb_re = -(P.l22 * nb + P.l12 * na) * 0.5f;
         const float pb_im = V + P.g22 * nb + P.g12 * na - P.detuning;
-        float sa, ca, sb, cb;
-        sincosf(pa_im * hdt, &sa, &ca);
-        sincosf(pb_im * hdt, &sb, &cb);
-        const float ma = expf(pa_re * hdt), mb = expf(pb_re * hdt);
-        da = make_float2(ma * ca, ma * sa);
-        db = make_float2(mb * cb, mb * sb);
+        const float2 ea = cis_small(pa_im * hdt), eb = cis_small(pb_im * hdt);
+        const float ma = exp_small(pa_re * hdt), mb = exp_small(pb_re * hdt);
+        da = make_float2(ma * ea.x, ma * ea.y);
+        db = make_float2(mb * eb.x, mb * eb.y);
         xa = cmul(a0, da);
         xb = cmul(b0, db);
     }

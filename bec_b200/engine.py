@@ -58,6 +58,8 @@ SIGNATURES = {
                                           _P(BecGsReport)]),
     "bec_warmstart_basis_size": (C.c_int32, []),
     "bec_pulse_finite": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    "bec_render_projections": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_float), _P(C.c_float), _P(C.c_float),
+                                         _P(C.c_float), _P(C.c_float), _P(C.c_float)]),
     "bec_mlp_create": (C.c_int, [_P(C.c_int32), C.c_int32, C.c_uint64, _P(C.c_void_p)]),
     "bec_mlp_destroy": (None, [C.c_void_p]),
     "bec_mlp_param_count": (C.c_int64, [C.c_void_p]),
@@ -260,6 +262,19 @@ class Engine:
                 off += 4 * d.nvz
             return mom, out
         return mom
+
+    def render_projections(self, group=0):
+        """RGBA images (float, h x w x 4) of the xy and zy projections of both components after a
+        pi/2 pulse, plus the projected densities: dict(xy_a, xy_b, zy_a, zy_b, levels_xy, levels_zy)."""
+        d = self.derived[group]
+        f = lambda *s: np.zeros(s, dtype=np.float32)
+        xy_a, xy_b = f(d.nvy, d.nvx, 4), f(d.nvy, d.nvx, 4)
+        zy_a, zy_b = f(d.nvy, d.nvz, 4), f(d.nvy, d.nvz, 4)
+        lxy, lzy = f(2, d.nvy, d.nvx), f(2, d.nvy, d.nvz)
+        p = lambda a: a.ctypes.data_as(_P(C.c_float))
+        self._check(lib().bec_render_projections(self._h, group, p(xy_a), p(xy_b), p(zy_a), p(zy_b), p(lxy), p(lzy)),
+                    "bec_render_projections")
+        return dict(xy_a=xy_a, xy_b=xy_b, zy_a=zy_a, zy_b=zy_b, levels_xy=lxy, levels_zy=lzy)
 
     def profile_steps(self, n_steps, max_classes=16):
         """Per grid class: dict(dims, traj, z_ms, plane_ms) mean device time per launch."""

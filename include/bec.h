@@ -254,6 +254,16 @@ bec_status bec_axial_now(bec_ctx *ctx, int32_t group, double *out);
  * ordered by group then index. */
 bec_status bec_traj_moments_now(bec_ctx *ctx, bec_moments *out);
 
+/* Headless version of the reference's state drawing (drawState, wigner.cu:413-430 with
+ * the projections of :384-410 and the colour ramp of spectre.cu:34-46): densities of both
+ * components after a pi/2 pulse about alpha = 0, Wigner term subtracted, summed over the
+ * group's trajectories and projected on xy (sum over z) and zy (sum over x), then mapped to
+ * RGBA floats with max levels 3 N ne nvz / (cells dV) (xy) and 3 N ne nvx / (cells dV) (zy).
+ * xy_*: nvy x nvx pixels, zy_*: nvy x nvz pixels, 4 floats each; levels_* (may be NULL) get
+ * the projected densities. Batched path only. */
+bec_status bec_render_projections(bec_ctx *ctx, int32_t group, float *xy_a, float *xy_b, float *zy_a,
+                                  float *zy_b, float *levels_xy, float *levels_zy);
+
 /* Runs a schedule. samples receives n_samples * n_groups moments
  * (sample-major), n_samples = n_steps / sample_every (or 1). When
  * schedule->axial is set, axial receives n_samples * sum_g(4 * nvz_g) doubles

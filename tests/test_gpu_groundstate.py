@@ -66,8 +66,10 @@ def test_batched_mu_rule_matches_oracle():
         psi_o, rep_o = O.ground_state(GROUPS[g], mode=BEC_GS_MU, max_steps=6000, tol=1e-6, check_every=20)
         assert reps[k].converged == 1 and rep_o.converged == 1
         assert abs(reps[k].steps - rep_o.steps) <= 20
-        assert reps[k].mu == pytest.approx(rep_o.mu, rel=1e-6)
         assert rel_state_err(outs[k], psi_o) < 1e-4
+        # mu still drifts by up to ~tol per check when the rule stops, so compare at the same step count
+        _, rep_f = O.ground_state(GROUPS[g], mode=BEC_GS_FIXED_STEPS, max_steps=reps[k].steps)
+        assert reps[k].mu == pytest.approx(rep_f.mu, rel=1e-6)
 
 
 def test_batched_warm_start_needs_fewer_steps():

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _oracle_finite(e, rabi_hz, duration, phi, dt):
-    n = max(1, int(round(duration / dt)))
+    n = max(1, int(np.floor(duration / dt + 0.5)))     # llround: halves round away from zero
     half = 0.5 * 2 * np.pi * rabi_hz * duration / n
     for _ in range(n):
         e.pulse(half, phi)
@@ -29,7 +29,7 @@ def test_finite_pulse_matches_oracle(path):
     eng.init_group(0, gs)
     e = O.OracleEnsemble(p)
     e.init(gs)
-    eng.pulse_finite(500.0, 0.5e-3, 0.3)      # 12.5 steps of 40 us -> 12 substeps
+    eng.pulse_finite(500.0, 0.5e-3, 0.3)      # 12.5 steps of 40 us -> 13 substeps
     _oracle_finite(e, 500.0, 0.5e-3, 0.3, p.dt_evo)
     eng.evolve(10)
     e.evolve(10)
