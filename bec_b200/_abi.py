@@ -27,6 +27,9 @@ BEC_PATH_FP32_BATCHED = 1
 BEC_GS_FIXED_STEPS = 0
 BEC_GS_MU = 1
 BEC_GS_REFERENCE_E = 2
+BEC_GS_MU_RESIDUAL = 3
+BEC_LR_CONSTANT = 0
+BEC_LR_COSINE = 1
 
 
 class BecParams(C.Structure):
@@ -79,6 +82,7 @@ class BecGsOpts(C.Structure):
         ("warm_per_group", C.c_int32),
         ("tol", C.c_double),
         ("warm_start", C.POINTER(C.c_double)),
+        ("res_tol", C.c_double),
     ]
 
 
@@ -87,6 +91,7 @@ class BecGsReport(C.Structure):
         ("steps", C.c_int32), ("converged", C.c_int32),
         ("mu", C.c_double), ("energy", C.c_double), ("N", C.c_double),
         ("residual", C.c_double), ("seconds", C.c_double),
+        ("step_residual", C.c_double),
     ]
 
 

@@ -94,6 +94,7 @@ struct bec_ctx {
     double last_ms = 0.0;
     long long last_launches = 0;
     std::vector<void *> allocs;
+    std::vector<WsTable> ws_tables;      // warm-start bases installed per grid
 };
 
 namespace {
@@ -722,6 +723,7 @@ void bec_destroy(bec_ctx *ctx)
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (void *p : ctx->allocs) cudaFree(p);
+    for (auto &t : ctx->ws_tables) cudaFree(t.d_basis);
     for (auto &gr : ctx->groups)
         if (gr.gs_dev) { /* owned through allocs */ }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -748,30 +750,33 @@ bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts
     if (!ctx) return BEC_ERR_INVALID_ARG;
     if (!opts || !psi_out || group < 0 || group >= (int)ctx->groups.size())
         return fail(ctx, BEC_ERR_INVALID_ARG, "bad ground-state arguments");
-    if (opts->mode < BEC_GS_FIXED_STEPS || opts->mode > BEC_GS_REFERENCE_E)
+    if (opts->mode < BEC_GS_FIXED_STEPS || opts->mode > BEC_GS_MU_RESIDUAL)
         return fail(ctx, BEC_ERR_INVALID_ARG, "unknown ground-state mode");
     GroupRec &gr = ctx->groups[group];
     const GeomD &g = gr.gd;
     const int cells = g.cells;
     cudaStream_t s = ctx->stream;
     const long long l0 = g_launches;
-    double2 *a = nullptr, *tmp = nullptr, *tmp2 = nullptr;
+    const bool mu_rule = opts->mode == BEC_GS_MU || opts->mode == BEC_GS_MU_RESIDUAL;
+    double2 *a = nullptr, *tmp = nullptr, *tmp2 = nullptr, *prev = nullptr;
     {
-        void *pa = nullptr, *pt = nullptr, *pt2 = nullptr;
+        void *pa = nullptr, *pt = nullptr, *pt2 = nullptr, *pp = nullptr;
         CKC(cudaMalloc(&pa, sizeof(double2) * cells));
         if (cudaMalloc(&pt, sizeof(double2) * cells) != cudaSuccess ||
-            cudaMalloc(&pt2, sizeof(double2) * cells) != cudaSuccess) {
-            cudaFree(pa); cudaFree(pt);
+            cudaMalloc(&pt2, sizeof(double2) * cells) != cudaSuccess ||
+            (mu_rule && cudaMalloc(&pp, sizeof(double2) * cells) != cudaSuccess)) {
+            cudaFree(pa); cudaFree(pt); cudaFree(pt2);
             return fail(ctx, BEC_ERR_OUT_OF_MEMORY, "ground-state buffers");
         }
-        a = (double2 *)pa; tmp = (double2 *)pt; tmp2 = (double2 *)pt2;
+        a = (double2 *)pa; tmp = (double2 *)pt; tmp2 = (double2 *)pt2; prev = (double2 *)pp;
     }
-    struct Guard { void *p[3]; ~Guard() { for (void *q : p) cudaFree(q); } } guard{{a, tmp, tmp2}};
+    struct Guard { void *p[4]; ~Guard() { for (void *q : p) cudaFree(q); } } guard{{a, tmp, tmp2, prev}};
     double *sc = ctx->d_scal;
     double *red = ctx->d_red;
     bec_status st;
 
     CKC(cudaEventRecord(ctx->ev0, s));
+    if (prev) CKC(cudaMemsetAsync(prev, 0, sizeof(double2) * cells, s));
     if (opts->warm_start) {
         CKC(cudaMemcpyAsync(a, opts->warm_start, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
     } else {
@@ -785,21 +790,25 @@ bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts
 
     const int maxs = opts->max_steps > 0 ? opts->max_steps : 1;
     const int check = opts->check_every > 0 ? opts->check_every : 1;
-    double E = 0.0, mu_prev = 0.0;
-    int steps = 0, converged = 0;
-    auto measure_mu = [&](double *mu_out) -> bec_status {
-        // x-space sums of the renormalised state, then the Parseval kinetic sum
+    double E = 0.0, mu_prev = 0.0, step_res = 0.0;
+    int steps = 0, converged = 0, checks = 0;
+    const double res_tol = opts->res_tol > 0.0 ? opts->res_tol : 10.0 * opts->tol;
+    auto measure_mu = [&](double *mu_out, double *diff) -> bec_status {
+        // x-space sums of the renormalised state, its change since the last check, the Parseval kinetic sum
         plain_gs_xsums(a, g, sc + 8, red, s);
+        plain_diff2(a, prev, cells, sc + 20, red, s);
+        CKC(cudaMemcpyAsync(prev, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
         CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
         bec_status st2 = plain_fft(ctx, tmp, g, 1);
         if (st2) return st2;
         plain_scale(tmp, cells, 1.0 / cells, s);
         plain_gs_ksum(tmp, g, sc + 12, red, s);
-        double h[8];
-        CKC(cudaMemcpyAsync(h, sc + 8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+        double h[14];
+        CKC(cudaMemcpyAsync(h, sc + 8, sizeof(double) * 14, cudaMemcpyDeviceToHost, s));
         CKC(cudaStreamSynchronize(s));
         const double ekin = h[4] * cells * g.dV, epot = h[0] * g.dV, eint = g.g11 * h[1] * g.dV, N = h[2] * g.dV;
         *mu_out = (ekin + epot + eint) / N;
+        *diff = std::sqrt(h[12] / h[13]);
         return BEC_OK;
     };
     while (steps < maxs) {
@@ -826,12 +835,16 @@ bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts
             const double newE = hE * g.dV;
             if (std::fabs((newE - E) / newE) < 0.000001) stop = true;   // :155
             E = newE;
-        } else if (opts->mode == BEC_GS_MU && (steps % check) == 0) {
-            double mu;
-            if ((st = measure_mu(&mu))) return st;
+        } else if (mu_rule && (steps % check) == 0) {
+            double mu, diff;
+            if ((st = measure_mu(&mu, &diff))) return st;
             if (!std::isfinite(mu)) return fail(ctx, BEC_ERR_NUMERICAL, "ground state diverged");
-            if (mu_prev != 0.0 && std::fabs((mu - mu_prev) / mu) < opts->tol) stop = true;
+            const double r = diff / ((double)check * gr.d.dt_steady * std::fabs(mu));
+            if (checks > 0) step_res = r;
+            const bool mu_ok = mu_prev != 0.0 && std::fabs((mu - mu_prev) / mu) < opts->tol;
+            if (mu_ok && (opts->mode == BEC_GS_MU || (checks > 0 && r < res_tol))) stop = true;
             mu_prev = mu;
+            ++checks;
         }
         if ((st = plain_fft(ctx, a, g, 1))) return st;                  // :151-152
         plain_scale(a, cells, 1.0 / cells, s);
@@ -848,6 +861,7 @@ bec_status bec_ground_state(bec_ctx *ctx, int32_t group, const bec_gs_opts *opts
         rep->steps = steps;
         rep->converged = converged;
         rep->seconds = ms * 1e-3;
+        rep->step_residual = step_res;
         // mu, energy, residual of the final state
         plain_gs_xsums(a, g, sc + 8, red, s);
         CKC(cudaMemcpyAsync(tmp, a, sizeof(double2) * cells, cudaMemcpyDeviceToDevice, s));
@@ -914,6 +928,8 @@ struct GsClass {
     std::vector<int> batch;            // its index in the caller's list
     float2 *state = nullptr, *out = nullptr, *warm = nullptr;
     int *d_tgroup = nullptr;
+    int *d_active = nullptr;           // class-local trajectories still iterating (device copy of active)
+    std::vector<int> active;
     double *norm = nullptr;            // [2][n]
     double *ekin = nullptr, *xsums = nullptr;
 };
@@ -921,8 +937,16 @@ struct GsClass {
 // Batched FP32 imaginary-time ground states for groups whose grids the register passes support.
 // psi_out (host states) may be NULL; coef_in (n x 64, host) seeds warm starts synthesised on the
 // device; coef_out (n x 64, host) receives the projections of the results on the correction basis.
+const WsTable *ws_table(const bec_ctx *ctx, int nx, int ny, int nz)
+{
+    for (const auto &t : ctx->ws_tables)
+        if (t.nx == nx && t.ny == ny && t.nz == nz) return &t;
+    return nullptr;
+}
+
 bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_opts *opts, double *const *psi_out,
-                      bec_gs_report *reports, const double *coef_in = nullptr, double *coef_out = nullptr)
+                      bec_gs_report *reports, const double *coef_in = nullptr, double *coef_out = nullptr,
+                      float *profile_out = nullptr)
 {
     cudaStream_t s = ctx->stream;
     const long long l0 = g_launches;
@@ -976,15 +1000,21 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
         CKC(talloc((void **)&d_gp, sizeof(GroupParamsF) * gfs.size()));
         CKC(cudaMemcpyAsync(d_gp, gfs.data(), sizeof(GroupParamsF) * gfs.size(), cudaMemcpyHostToDevice, s));
     }
+    CKC(cudaEventRecord(ctx->ev0, s));      // the timed region includes the warm-start synthesis
     for (auto &c : cls) {
         const size_t nt = c.groups.size(), cells = c.geom.cells;
         c.geom.n_traj = (int)nt;
         CKC(talloc((void **)&c.state, sizeof(float2) * nt * cells));
         CKC(talloc((void **)&c.out, sizeof(float2) * nt * cells));
         CKC(talloc((void **)&c.d_tgroup, sizeof(int) * nt));
+        CKC(talloc((void **)&c.d_active, sizeof(int) * nt));
+        c.active.resize(nt);
+        for (size_t t = 0; t < nt; ++t) c.active[t] = (int)t;
+        CKC(cudaMemcpyAsync(c.d_active, c.active.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
         CKC(talloc((void **)&c.norm, sizeof(double) * 2 * nt));
         CKC(talloc((void **)&c.ekin, sizeof(double) * nt));
-        CKC(talloc((void **)&c.xsums, sizeof(double) * 3 * nt));
+        CKC(talloc((void **)&c.xsums, sizeof(double) * 4 * nt));
+        CKC(cudaMemsetAsync(c.out, 0, sizeof(float2) * nt * cells, s));   // the first check sees a full change
         CKC(cudaMemcpyAsync(c.d_tgroup, c.groups.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
         CKC(cudaMemsetAsync(c.norm, 0, sizeof(double) * 2 * nt, s));
         if (opts->warm_start) {
@@ -1005,12 +1035,12 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
                 for (int k = 0; k < nb; ++k) cc[t * nb + k] = coef_in[(size_t)c.batch[t] * nb + k];
             }
             CKC(talloc((void **)&c.warm, sizeof(float2) * nt * cells));
-            CKC(warmstart_synth(cc.data(), (int)nt, dd.data(), c.warm, s));
+            CKC(warmstart_synth(cc.data(), (int)nt, dd.data(), ws_table(ctx, c.geom.nx, c.geom.ny, c.geom.nz),
+                                c.warm, s));
         }
     }
     auto tw_for = [&](int nz, float2 **tw) { return get_tw32_full(ctx, nz, tw); };
     bec_status st;
-    CKC(cudaEventRecord(ctx->ev0, s));
     // start: x-space profile -> stored form; measure its norm, first half kick of step 0
     for (auto &c : cls) {
         float2 *tw;
@@ -1023,49 +1053,59 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
     CKL();
     const int maxs = opts->max_steps > 0 ? opts->max_steps : 1;
     const int check = opts->check_every > 0 ? opts->check_every : 1;
-    const bool mu_mode = opts->mode == BEC_GS_MU;
-    std::vector<std::vector<double>> mu_prev(cls.size()), conv_step(cls.size());
+    const bool mu_mode = opts->mode == BEC_GS_MU || opts->mode == BEC_GS_MU_RESIDUAL;
+    const double res_tol = opts->res_tol > 0.0 ? opts->res_tol : 10.0 * opts->tol;
+    std::vector<std::vector<double>> mu_prev(cls.size()), conv_step(cls.size()), step_res(cls.size());
     for (size_t k = 0; k < cls.size(); ++k) {
         mu_prev[k].assign(cls[k].groups.size(), 0.0);
         conv_step[k].assign(cls[k].groups.size(), -1.0);
+        step_res[k].assign(cls[k].groups.size(), 0.0);
     }
-    int steps = 0;
+    int steps = 0, checks = 0;
     bool converged_all = false;
-    // measures the boundary state after `steps` steps: writes out (renormalised x-space) and mu per trajectory
-    auto boundary = [&](bool final_pass, std::vector<std::vector<double>> *mus) -> bec_status {
+    // measures the boundary state after `steps` steps: writes out (renormalised x-space), mu per trajectory
+    // and the relative change of the state since the previous boundary
+    // launches cover the active trajectories only; per-trajectory buffers stay indexed by class-local position
+    auto run_geom = [](const GsClass &c) { ClassGeom g = c.geom; g.n_traj = (int)c.active.size(); return g; };
+    auto boundary = [&](bool final_pass, std::vector<std::vector<double>> *mus,
+                        std::vector<std::vector<double>> *diffs) -> bec_status {
         const int b = steps & 1;            // buffer the closing pencil pass measures into
         for (auto &c : cls) {
+            if (c.active.empty()) continue;
             float2 *tw;
             bec_status st2;
             if ((st2 = tw_for(c.geom.nz, &tw))) return st2;
             const int nt = c.geom.n_traj;
+            const ClassGeom ag = run_geom(c);
             CKC(cudaMemsetAsync(c.ekin, 0, sizeof(double) * nt, s));
-            CKC(cudaMemsetAsync(c.xsums, 0, sizeof(double) * 3 * nt, s));
-            gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.0f, 1.0f / c.geom.cells,
-                      (float)(c.geom.nx * c.geom.ny), c.norm + (size_t)b * nt, c.ekin, s);
-            gs_output(c.state, c.geom, d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt, c.out, c.xsums,
-                      1.0f / (float)(c.geom.nx * c.geom.ny), s);
+            CKC(cudaMemsetAsync(c.xsums, 0, sizeof(double) * 4 * nt, s));
+            gs_pencil(c.state, ag, d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.0f, 1.0f / c.geom.cells,
+                      (float)(c.geom.nx * c.geom.ny), c.norm + (size_t)b * nt, c.ekin, s, c.d_active);
+            gs_output(c.state, ag, d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt, c.out, c.xsums,
+                      1.0f / (float)(c.geom.nx * c.geom.ny), s, c.d_active);
             if (!final_pass)   // resume: first half kick of the next step, norm already measured
-                gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.0f, 0.5f, 1.0f / c.geom.cells, 1.0f,
-                          nullptr, nullptr, s);
+                gs_pencil(c.state, ag, d_gp, d_gs, c.d_tgroup, tw, 0.0f, 0.5f, 1.0f / c.geom.cells, 1.0f,
+                          nullptr, nullptr, s, c.d_active);
         }
         CKL();
         if (mus) {
             for (size_t k = 0; k < cls.size(); ++k) {
                 auto &c = cls[k];
                 const int nt = c.geom.n_traj;
-                std::vector<double> nrm(nt), ek(nt), xs(3 * nt);
+                std::vector<double> nrm(nt), ek(nt), xs(4 * nt);
                 CKC(cudaMemcpyAsync(nrm.data(), c.norm + (size_t)b * nt, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
                 CKC(cudaMemcpyAsync(ek.data(), c.ekin, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
-                CKC(cudaMemcpyAsync(xs.data(), c.xsums, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, s));
+                CKC(cudaMemcpyAsync(xs.data(), c.xsums, sizeof(double) * 4 * nt, cudaMemcpyDeviceToHost, s));
                 CKC(cudaStreamSynchronize(s));
-                (*mus)[k].resize(nt);
-                for (int t = 0; t < nt; ++t) {
+                (*mus)[k].assign(nt, 0.0);
+                (*diffs)[k].assign(nt, 0.0);
+                for (int t : c.active) {
                     const bec_derived &d = ctx->groups[c.groups[t]].d;
                     const double s2 = d.N / (nrm[t] * (double)d.cells * d.dV);       // renormalisation squared
                     const double e_kin = ek[t] * s2 * (double)d.cells * d.dV;
-                    const double N = xs[3 * t + 2] * d.dV;
-                    (*mus)[k][t] = (e_kin + xs[3 * t] * d.dV + d.g11 * xs[3 * t + 1] * d.dV) / N;
+                    const double N = xs[4 * t + 2] * d.dV;
+                    (*mus)[k][t] = (e_kin + xs[4 * t] * d.dV + d.g11 * xs[4 * t + 1] * d.dV) / N;
+                    (*diffs)[k][t] = std::sqrt(xs[4 * t + 3] / xs[4 * t + 2]);
                 }
             }
         }
@@ -1074,40 +1114,59 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
     while (steps < maxs) {
         const int b = steps & 1;
         for (auto &c : cls) {
+            if (c.active.empty()) continue;
             const int nt = c.geom.n_traj;
-            gs_plane_step(c.state, c.geom, d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt,
-                          c.norm + (size_t)(b ^ 1) * nt, s);
+            gs_plane_step(c.state, run_geom(c), d_gp, d_gs, c.d_tgroup, c.norm + (size_t)b * nt,
+                          c.norm + (size_t)(b ^ 1) * nt, s, c.d_active);
         }
         CKL();
         ++steps;
         const bool last = steps == maxs;
         if (mu_mode && (steps % check) == 0 && !last) {
-            std::vector<std::vector<double>> mus(cls.size());
-            if ((st = boundary(false, &mus))) return st;
+            std::vector<std::vector<double>> mus(cls.size()), diffs(cls.size());
+            if ((st = boundary(false, &mus, &diffs))) return st;
             bool all = true;
-            for (size_t k = 0; k < cls.size(); ++k)
-                for (size_t t = 0; t < mus[k].size(); ++t) {
+            for (size_t k = 0; k < cls.size(); ++k) {
+                for (int t : cls[k].active) {
                     const double m = mus[k][t];
                     if (!std::isfinite(m)) return fail(ctx, BEC_ERR_NUMERICAL, "ground state diverged");
-                    if (conv_step[k][t] < 0 && mu_prev[k][t] != 0.0 && std::fabs((m - mu_prev[k][t]) / m) < opts->tol)
+                    const double dt = ctx->groups[cls[k].groups[t]].d.dt_steady;
+                    const double r = diffs[k][t] / ((double)check * dt * std::fabs(m));
+                    if (checks > 0) step_res[k][t] = r;
+                    const bool mu_ok = mu_prev[k][t] != 0.0 && std::fabs((m - mu_prev[k][t]) / m) < opts->tol;
+                    if (conv_step[k][t] < 0 && mu_ok &&
+                        (opts->mode == BEC_GS_MU || (checks > 0 && r < res_tol)))
                         conv_step[k][t] = steps;
                     mu_prev[k][t] = m;
-                    all = all && conv_step[k][t] >= 0;
                 }
+                // converged trajectories leave the batch; their out keeps the state they converged in
+                std::vector<int> still;
+                for (int t : cls[k].active)
+                    if (conv_step[k][t] < 0) still.push_back(t);
+                if (still.size() != cls[k].active.size()) {
+                    cls[k].active = still;
+                    if (!still.empty())
+                        CKC(cudaMemcpyAsync(cls[k].d_active, still.data(), sizeof(int) * still.size(),
+                                            cudaMemcpyHostToDevice, s));
+                }
+                all = all && cls[k].active.empty();
+            }
+            ++checks;
             if (all) { converged_all = true; break; }
         } else if (!last) {
             for (auto &c : cls) {
+                if (c.active.empty()) continue;
                 float2 *tw;
                 if ((st = tw_for(c.geom.nz, &tw))) return st;
                 const int nt = c.geom.n_traj;
-                gs_pencil(c.state, c.geom, d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.5f, 1.0f / c.geom.cells, 1.0f,
-                          c.norm + (size_t)((steps & 1)) * nt, nullptr, s);
+                gs_pencil(c.state, run_geom(c), d_gp, d_gs, c.d_tgroup, tw, 0.5f, 0.5f, 1.0f / c.geom.cells, 1.0f,
+                          c.norm + (size_t)((steps & 1)) * nt, nullptr, s, c.d_active);
             }
             CKL();
         }
     }
-    // after a check at which every trajectory converged, out already holds the renormalised boundary state
-    if (!converged_all && (st = boundary(true, nullptr))) return st;
+    // trajectories that converged at a check already hold their renormalised state in out
+    if (!converged_all && (st = boundary(true, nullptr, nullptr))) return st;
     CKC(cudaEventRecord(ctx->ev1, s));
     CKC(cudaEventSynchronize(ctx->ev1));
     float ms = 0.f;
@@ -1135,21 +1194,28 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
             const double cs = conv_step[cls_of[i]][idx_in[i]];
             r.converged = mu_mode ? (cs >= 0 ? 1 : 0) : 0;
             r.steps = (mu_mode && cs >= 0) ? (int)cs : steps;
+            r.step_residual = step_res[cls_of[i]][idx_in[i]];
             r.seconds = ms * 1e-3;
             gs_to_double(src, a64, cells, s);
             if ((st = plain_measures(ctx, ctx->groups[groups[i]].gd, a64, t1, t2, &r))) return st;
         }
     }
-    if (coef_out) {
+    if (coef_out || profile_out) {
         const int nb = warmstart_basis_size();
         for (auto &c : cls) {
-            const size_t nt = c.groups.size();
+            const size_t nt = c.groups.size(), cells = c.geom.cells;
             std::vector<bec_derived> dd(nt);
             for (size_t t = 0; t < nt; ++t) dd[t] = ctx->groups[c.groups[t]].d;
             std::vector<double> cc(nt * nb);
-            CKC(warmstart_project(c.out, (int)nt, dd.data(), cc.data(), s));
-            for (size_t t = 0; t < nt; ++t)
-                for (int k = 0; k < nb; ++k) coef_out[(size_t)c.batch[t] * nb + k] = cc[t * nb + k];
+            std::vector<float> pr(profile_out ? nt * cells : 0);
+            CKC(warmstart_project(c.out, (int)nt, dd.data(), ws_table(ctx, c.geom.nx, c.geom.ny, c.geom.nz),
+                                  coef_out ? cc.data() : nullptr, profile_out ? pr.data() : nullptr, s));
+            for (size_t t = 0; t < nt; ++t) {
+                if (coef_out)
+                    for (int k = 0; k < nb; ++k) coef_out[(size_t)c.batch[t] * nb + k] = cc[t * nb + k];
+                if (profile_out)
+                    std::memcpy(profile_out + (size_t)c.batch[t] * cells, pr.data() + t * cells, sizeof(float) * cells);
+            }
         }
     }
     ctx->last_launches = g_launches - l0;
@@ -1160,11 +1226,14 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
 } // namespace
 
 bec_status bec_ground_state_coeffs(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
-                                   const double *coef_in, double *coef_out, bec_gs_report *reports)
+                                   const double *coef_in, double *coef_out, float *profile_out,
+                                   bec_gs_report *reports)
 {
     if (!ctx || n < 1 || !groups || !opts) return BEC_ERR_INVALID_ARG;
+    if (opts->mode < BEC_GS_FIXED_STEPS || opts->mode > BEC_GS_MU_RESIDUAL)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "unknown ground-state mode");
     if (ctx->path != BEC_PATH_FP32_BATCHED || opts->mode == BEC_GS_REFERENCE_E || opts->warm_start)
-        return fail(ctx, BEC_ERR_INVALID_ARG, "coefficient ground states need the batched path, FIXED or MU rules");
+        return fail(ctx, BEC_ERR_INVALID_ARG, "coefficient ground states need the batched path and a FIXED or MU rule");
     const bec_derived &d0 = ctx->groups[groups[0]].d;
     for (int i = 0; i < n; ++i) {
         if (groups[i] < 0 || groups[i] >= (int)ctx->groups.size()) return fail(ctx, BEC_ERR_INVALID_ARG, "bad group");
@@ -1174,19 +1243,51 @@ bec_status bec_ground_state_coeffs(bec_ctx *ctx, int32_t n, const int32_t *group
         if (d.nvx != d0.nvx || d.nvy != d0.nvy || d.nvz != d0.nvz || !gs_batched_supported(g))
             return fail(ctx, BEC_ERR_UNSUPPORTED_GRID, "coefficient ground states need one supported grid");
     }
-    return gs_batched(ctx, n, groups, opts, nullptr, reports, coef_in, coef_out);
+    return gs_batched(ctx, n, groups, opts, nullptr, reports, coef_in, coef_out, profile_out);
 }
 
 int32_t bec_warmstart_basis_size(void) { return warmstart_basis_size(); }
+
+bec_status bec_warmstart_set_basis(bec_ctx *ctx, int32_t nvx, int32_t nvy, int32_t nvz, int32_t nb,
+                                   const float *basis)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (nvx < 2 || nvy < 1 || nvz < 2 || (nvx & (nvx - 1)) || (nvy & (nvy - 1)) || (nvz & (nvz - 1)) || nb < 0 ||
+        nb > warmstart_basis_size() || (nb > 0 && !basis))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad warm-start basis arguments");
+    for (size_t i = 0; i < ctx->ws_tables.size(); ++i) {
+        WsTable &t = ctx->ws_tables[i];
+        if (t.nx == nvx && t.ny == nvy && t.nz == nvz) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(t.d_basis);
+            ctx->ws_tables.erase(ctx->ws_tables.begin() + i);
+            break;
+        }
+    }
+    if (nb == 0 || !basis) return BEC_OK;
+    WsTable t;
+    t.nx = nvx; t.ny = nvy; t.nz = nvz; t.nb = nb;
+    const cudaError_t e = warmstart_table_init(t, basis, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(t.d_basis);
+        if (e == cudaErrorInvalidValue) return fail(ctx, BEC_ERR_INVALID_ARG, "warm-start basis rows are dependent");
+        return fail(ctx, e == cudaErrorMemoryAllocation ? BEC_ERR_OUT_OF_MEMORY : BEC_ERR_CUDA,
+                    std::string("warm-start basis: ") + cudaGetErrorString(e));
+    }
+    ctx->ws_tables.push_back(t);
+    return BEC_OK;
+}
 
 bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
                                   double *const *psi_out, bec_gs_report *reports)
 {
     if (!ctx || n < 0 || (n > 0 && (!groups || !psi_out || !opts))) return BEC_ERR_INVALID_ARG;
+    if (n > 0 && (opts->mode < BEC_GS_FIXED_STEPS || opts->mode > BEC_GS_MU_RESIDUAL))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "unknown ground-state mode");
     for (int i = 0; i < n; ++i)
         if (groups[i] < 0 || groups[i] >= (int)ctx->groups.size() || !psi_out[i])
             return fail(ctx, BEC_ERR_INVALID_ARG, "bad group index or output pointer");
-    // the batched FP32 path: FIXED_STEPS or MU rules on grids the register passes cover
+    // the batched FP32 path: FIXED_STEPS, MU or MU_RESIDUAL rules on grids the register passes cover
     bool batched = ctx->path == BEC_PATH_FP32_BATCHED && opts->mode != BEC_GS_REFERENCE_E && n > 0;
     for (int i = 0; batched && i < n; ++i) {
         const bec_derived &d = ctx->groups[groups[i]].d;

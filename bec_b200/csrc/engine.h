@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/bec.h"
 
 // ----------------------------------------------------------------------------
@@ -62,6 +64,8 @@ void plain_norm(const double2 *a, int n, double *out, double *tmp, cudaStream_t 
 void plain_renorm(double2 *a, int n, const double *sum, double N, double dV, cudaStream_t s);
 // x-space sums: out[0] = sum n V, out[1] = sum n^2, out[2] = sum n
 void plain_gs_xsums(const double2 *a, const GeomD &g, double *out, double *tmp, cudaStream_t s);
+// out[0] = sum |a - prev|^2, out[1] = sum |a|^2
+void plain_diff2(const double2 *a, const double2 *prev, int n, double *out, double *tmp, cudaStream_t s);
 // k-space sum of |ak|^2 k^2/2 into out[0]
 void plain_gs_ksum(const double2 *ak, const GeomD &g, double *out, double *tmp, cudaStream_t s);
 // reference energy integrand sum (wigner_kernel.cu:232-258) into out[0]
@@ -121,22 +125,35 @@ void gs_init(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const Gs
              const float2 *warm, cudaStream_t s);
 void gs_prep(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
              cudaStream_t s);
+// active (device, c.n_traj entries, may be NULL = 0 .. n_traj-1): the class-local trajectories this launch
+// processes, so converged trajectories can leave the batch
 void gs_plane_step(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
-                   const double *norm_in, double *norm_clear, cudaStream_t s);
-// FFT_xy of the stored state times in_scale * sqrt(N / N'): x-space rows to out, sums (n V, n^2, n) to xsums
+                   const double *norm_in, double *norm_clear, cudaStream_t s, const int *active = nullptr);
+// FFT_xy of the stored state times in_scale * sqrt(N / N'): x-space rows to out, sums (n V, n^2, n,
+// |u - previous out|^2) to xsums[4 traj ..]
 void gs_output(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
-               const double *norm_in, float2 *out, double *xsums, float in_scale, cudaStream_t s);
+               const double *norm_in, float2 *out, double *xsums, float in_scale, cudaStream_t s,
+               const int *active = nullptr);
 // kick exp(-dt frac1 k^2/2) * scale [measure] then exp(-dt frac2 k^2/2) * out_scale
 void gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
                const float2 *tw_full, float frac1, float frac2, float scale, float out_scale, double *norm,
-               double *ekin, cudaStream_t s);
+               double *ekin, cudaStream_t s, const int *active = nullptr);
 
 void gs_to_double(const float2 *in, double2 *out, size_t n, cudaStream_t s);
 
-// warmstart.cu: the 64-term correction over Thomas-Fermi (one grid per call)
+// warmstart.cu: the 64-term correction over Thomas-Fermi (one grid per call), from the
+// built-in analytic basis or from a table of basis rows installed for that grid
+struct WsTable {
+    int nx = 0, ny = 0, nz = 0, nb = 0;
+    float *d_basis = nullptr;          // nb x cells, grid index order
+    std::vector<double> gram;          // 64 x 64 Gram matrix (the identity beyond nb)
+};
 int warmstart_basis_size();
-cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, double *coef_out, cudaStream_t s);
-cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, float2 *psi_out, cudaStream_t s);
+cudaError_t warmstart_table_init(WsTable &t, const float *host_basis, cudaStream_t s);
+cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, const WsTable *tab, double *coef_out,
+                              float *profile_out, cudaStream_t s);
+cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, const WsTable *tab, float2 *psi_out,
+                            cudaStream_t s);
 
 // render.cu: projections after the reference's second pi/2 and the colour ramp
 void render_project(const float4 *x, const ClassGeom &c, float in_scale, float sub, float *xy_a, float *xy_b,

@@ -35,7 +35,8 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
                                                   int tiles, const GroupParamsF *__restrict__ gp,
                                                   const GsParamsF *__restrict__ gs, const int *__restrict__ tgroup,
                                                   const float2 *__restrict__ tw_g, GsArgs a,
-                                                  double *__restrict__ norm, double *__restrict__ ekin)
+                                                  double *__restrict__ norm, double *__restrict__ ekin,
+                                                  const int *__restrict__ active)
 {
     constexpr int R = 16, G = NZ / 16;
     extern __shared__ float2 dyn2[];
@@ -46,8 +47,9 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
     __shared__ double red[2][NZ / 32];
 
     const int t = threadIdx.x;
-    const int traj = blockIdx.x / tiles;
-    const int pen0 = (blockIdx.x - traj * tiles) * 16;
+    const int lt = blockIdx.x / tiles;                   // position in the launch's trajectory list
+    const int traj = active ? active[lt] : lt;
+    const int pen0 = (blockIdx.x - lt * tiles) * 16;
     const int gi = tgroup[traj];
     const GroupParamsF P = gp[gi];
     const float dts = gs[gi].dt_steady;
@@ -153,7 +155,8 @@ __global__ void __launch_bounds__(128) k_gs_plane(float2 *__restrict__ state, in
                                                   const GroupParamsF *__restrict__ gp,
                                                   const GsParamsF *__restrict__ gs, const int *__restrict__ tgroup,
                                                   const double *__restrict__ norm_in, double *__restrict__ norm_clear,
-                                                  float2 *__restrict__ out, double *__restrict__ xsums, float in_scale)
+                                                  float2 *__restrict__ out, double *__restrict__ xsums, float in_scale,
+                                                  const int *__restrict__ active)
 {
     constexpr int W = 32 / N;
     constexpr int PLANE = N * N;
@@ -162,7 +165,8 @@ __global__ void __launch_bounds__(128) k_gs_plane(float2 *__restrict__ state, in
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wp = lane / N, c = lane % N;
     const int plane_id = (blockIdx.x * 4 + warp) * W + wp;
-    const int traj = plane_id / nz, z = plane_id - traj * nz;
+    const int lt = plane_id / nz, z = plane_id - lt * nz;
+    const int traj = active ? active[lt] : lt;
     float2 *__restrict__ g = state + (size_t)traj * cells + (size_t)z * PLANE;
     float2 *s = tile2 + (warp * W + wp) * PLANE;
     const int gi = tgroup[traj];
@@ -234,28 +238,34 @@ __global__ void __launch_bounds__(128) k_gs_plane(float2 *__restrict__ state, in
         const float Y = -P.ymax + P.dy * (float)c;
         const float Z = -P.zmax + P.dz * (float)z;
         const float base = Y * Y + Z * Z * P.inv_lambda2;
-        double sv = 0.0, s2 = 0.0, s1 = 0.0;
+        // sums: n V, n^2, n and |u - previous output|^2 (the state's change since the last output)
+        double sv = 0.0, s2 = 0.0, s1 = 0.0, sd = 0.0;
         float2 *o = out + (size_t)traj * cells + (size_t)z * PLANE + c * N;
 #pragma unroll
         for (int x = 0; x < N; ++x) {
             const float2 u = make_float2(v[x].x * scale, v[x].y * scale);
+            const float2 w = o[x];
             o[x] = u;
             const float X = -P.xmax + P.dx * (float)x;
             const double n = (double)u.x * u.x + (double)u.y * u.y;
+            const float ex = u.x - w.x, ey = u.y - w.y;
             sv += n * (double)(0.5f * (X * X + base));
             s2 += n * n;
             s1 += n;
+            sd += (double)(ex * ex + ey * ey);
         }
         if (xsums) {
             for (int off = N / 2; off > 0; off >>= 1) {
                 sv += __shfl_down_sync(0xffffffffu, sv, off, N);
                 s2 += __shfl_down_sync(0xffffffffu, s2, off, N);
                 s1 += __shfl_down_sync(0xffffffffu, s1, off, N);
+                sd += __shfl_down_sync(0xffffffffu, sd, off, N);
             }
             if (c == 0) {
-                atomicAdd(xsums + 3 * traj + 0, sv);
-                atomicAdd(xsums + 3 * traj + 1, s2);
-                atomicAdd(xsums + 3 * traj + 2, s1);
+                atomicAdd(xsums + 4 * traj + 0, sv);
+                atomicAdd(xsums + 4 * traj + 1, s2);
+                atomicAdd(xsums + 4 * traj + 2, s1);
+                atomicAdd(xsums + 4 * traj + 3, sd);
             }
         }
     } else {
@@ -286,7 +296,7 @@ __global__ void k_gs_init(float2 *state, int nx, int lx, int ny, int ly, int cel
 template <int N, int MODE>
 void launch_gs_plane(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs,
                      const int *tgroup, const double *norm_in, double *norm_clear, float2 *out, double *xsums,
-                     float in_scale, cudaStream_t s)
+                     float in_scale, const int *active, cudaStream_t s)
 {
     constexpr int W = 32 / N;
     const size_t smem = sizeof(float2) * 4 * W * N * N;
@@ -296,14 +306,14 @@ void launch_gs_plane(float2 *state, const ClassGeom &c, const GroupParamsF *gp, 
         attr = true;
     }
     k_gs_plane<N, MODE><<<c.n_traj * c.nz / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, gs, tgroup, norm_in,
-                                                                      norm_clear, out, xsums, in_scale);
+                                                                      norm_clear, out, xsums, in_scale, active);
     g_launches++;
 }
 
 template <int NZ>
 void launch_gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs,
                       const int *tgroup, const float2 *tw, const GsArgs &a, double *norm, double *ekin,
-                      cudaStream_t s)
+                      const int *active, cudaStream_t s)
 {
     const int tiles = c.nx * c.ny / 16;
     const size_t smem = sizeof(float2) * (16 * NZ + NZ) + sizeof(float) * (NZ + 16);
@@ -313,19 +323,19 @@ void launch_gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp,
         attr = true;
     }
     k_gs_pencil<NZ><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, gs, tgroup, tw,
-                                                       a, norm, ekin);
+                                                       a, norm, ekin, active);
     g_launches++;
 }
 
 template <int MODE>
 void dispatch_plane(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
                     const double *norm_in, double *norm_clear, float2 *out, double *xsums, float in_scale,
-                    cudaStream_t s)
+                    const int *active, cudaStream_t s)
 {
     switch (c.nx) {
-    case 8: launch_gs_plane<8, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, s); break;
-    case 16: launch_gs_plane<16, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, s); break;
-    case 32: launch_gs_plane<32, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, s); break;
+    case 8: launch_gs_plane<8, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, active, s); break;
+    case 16: launch_gs_plane<16, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, active, s); break;
+    case 32: launch_gs_plane<32, MODE>(state, c, gp, gs, tgroup, norm_in, norm_clear, out, xsums, in_scale, active, s); break;
     default: break;
     }
 }
@@ -366,30 +376,30 @@ void gs_init(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const Gs
 void gs_prep(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
              cudaStream_t s)
 {
-    dispatch_plane<1>(state, c, gp, gs, tgroup, nullptr, nullptr, nullptr, nullptr, 1.0f, s);
+    dispatch_plane<1>(state, c, gp, gs, tgroup, nullptr, nullptr, nullptr, nullptr, 1.0f, nullptr, s);
 }
 
 void gs_plane_step(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
-                   const double *norm_in, double *norm_clear, cudaStream_t s)
+                   const double *norm_in, double *norm_clear, cudaStream_t s, const int *active)
 {
-    dispatch_plane<0>(state, c, gp, gs, tgroup, norm_in, norm_clear, nullptr, nullptr, 1.0f, s);
+    dispatch_plane<0>(state, c, gp, gs, tgroup, norm_in, norm_clear, nullptr, nullptr, 1.0f, active, s);
 }
 
 void gs_output(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
-               const double *norm_in, float2 *out, double *xsums, float in_scale, cudaStream_t s)
+               const double *norm_in, float2 *out, double *xsums, float in_scale, cudaStream_t s, const int *active)
 {
-    dispatch_plane<2>(state, c, gp, gs, tgroup, norm_in, nullptr, out, xsums, in_scale, s);
+    dispatch_plane<2>(state, c, gp, gs, tgroup, norm_in, nullptr, out, xsums, in_scale, active, s);
 }
 
 void gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp, const GsParamsF *gs, const int *tgroup,
                const float2 *tw_full, float frac1, float frac2, float scale, float out_scale, double *norm,
-               double *ekin, cudaStream_t s)
+               double *ekin, cudaStream_t s, const int *active)
 {
     GsArgs a{frac1, frac2, scale, out_scale, norm ? 1 : 0};
     switch (c.nz) {
-    case 64: launch_gs_pencil<64>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, s); break;
-    case 128: launch_gs_pencil<128>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, s); break;
-    case 256: launch_gs_pencil<256>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, s); break;
+    case 64: launch_gs_pencil<64>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, active, s); break;
+    case 128: launch_gs_pencil<128>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, active, s); break;
+    case 256: launch_gs_pencil<256>(state, c, gp, gs, tgroup, tw_full, a, norm, ekin, active, s); break;
     default: break;
     }
 }

@@ -458,26 +458,29 @@ bec_status bec_mlp_gradients(bec_mlp *m, const float *x, const float *target, in
     return BEC_OK;
 }
 
-// Adam on minibatches drawn (seeded) from n samples; loss_history[s] = loss of step s.
+// Adam on minibatches drawn (seeded) from n samples; loss_history[s] = loss of step s. Every
+// minibatch's indices are drawn up front and uploaded once, and the losses stay on the device
+// until the end, so the step loop issues work without waiting on the GPU.
 bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_t n, int32_t batch, int32_t steps,
-                         float lr, uint64_t seed, float *loss_history)
+                         float lr, int32_t schedule, uint64_t seed, float *loss_history)
 {
     if (!m || !x || !target || n < 1 || batch < 1 || steps < 0) return BEC_ERR_INVALID_ARG;
+    if (schedule != BEC_LR_CONSTANT && schedule != BEC_LR_COSINE) return BEC_ERR_INVALID_ARG;
     const int rows = round_up(batch, 64);
     bec_status st;
     if ((st = mlp_reserve(m, rows))) return st;
     const int in_r = m->w_real[0], out_r = m->w_real[m->L], inw = m->w[0], ow = m->w[m->L];
-    float *dx = nullptr, *dt = nullptr;
+    float *dx = nullptr, *dt = nullptr, *dhist = nullptr;
     int *didx = nullptr;
     std::vector<void *> loc;
     auto lalloc = [&](void **p, size_t b) {
-        cudaError_t e = cudaMalloc(p, b);
+        cudaError_t e = cudaMalloc(p, b > 0 ? b : 16);
         if (e == cudaSuccess) loc.push_back(*p);
         return e;
     };
     struct F { std::vector<void *> &v; cudaStream_t s; ~F() { cudaStreamSynchronize(s); for (void *p : v) cudaFree(p); } } f{loc, m->s};
     if (lalloc((void **)&dx, sizeof(float) * (size_t)n * inw) || lalloc((void **)&dt, sizeof(float) * (size_t)n * ow) ||
-        lalloc((void **)&didx, sizeof(int) * rows))
+        lalloc((void **)&didx, sizeof(int) * (size_t)rows * steps) || lalloc((void **)&dhist, sizeof(float) * steps))
         return BEC_ERR_OUT_OF_MEMORY;
     {
         std::vector<float> hx((size_t)n * inw, 0.0f), ht((size_t)n * ow, 0.0f);
@@ -488,33 +491,38 @@ bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_
         cudaMemcpy(dx, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice);
         cudaMemcpy(dt, ht.data(), sizeof(float) * ht.size(), cudaMemcpyHostToDevice);
     }
+    // minibatches: consecutive slices of seeded shuffles of the n samples
     std::mt19937_64 rng(seed);
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     int pos = n;
-    std::vector<int> hidx(rows, 0);
     const int valid = std::min(batch, n);
-    std::vector<float> hist(steps, 0.0f);
-    for (int s = 0; s < steps; ++s) {
+    std::vector<int> hidx((size_t)rows * steps, 0);
+    for (int s = 0; s < steps; ++s)
         for (int r = 0; r < valid; ++r) {
             if (pos >= n) { std::shuffle(order.begin(), order.end(), rng); pos = 0; }
-            hidx[r] = order[pos++];
+            hidx[(size_t)s * rows + r] = order[pos++];
         }
-        cudaMemcpyAsync(didx, hidx.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, m->s);
-        k_gather<<<grid_for((size_t)rows * inw), 256, 0, m->s>>>(dx, didx, m->y[0], rows, valid, inw);
-        k_gather<<<grid_for((size_t)rows * ow), 256, 0, m->s>>>(dt, didx, m->tgt, rows, valid, ow);
+    if (steps > 0) cudaMemcpy(didx, hidx.data(), sizeof(int) * hidx.size(), cudaMemcpyHostToDevice);
+    const double pi = 3.14159265358979323846;
+    for (int s = 0; s < steps; ++s) {
+        const int *bidx = didx + (size_t)s * rows;
+        k_gather<<<grid_for((size_t)rows * inw), 256, 0, m->s>>>(dx, bidx, m->y[0], rows, valid, inw);
+        k_gather<<<grid_for((size_t)rows * ow), 256, 0, m->s>>>(dt, bidx, m->tgt, rows, valid, ow);
         mlp_forward_dev(m, rows);
         mlp_backward_dev(m, rows, valid);
         ++m->adam_t;
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = 1.0f - std::pow(b1, (float)m->adam_t), c2 = 1.0f - std::pow(b2, (float)m->adam_t);
-        k_adam<<<grid_for(m->n_params), 256, 0, m->s>>>(m->p, m->m, m->v, m->g, m->n_params, lr, b1, b2, 1e-8f, c1, c2);
+        const float lr_s = schedule == BEC_LR_COSINE ? (float)(lr * 0.5 * (1.0 + std::cos(pi * s / steps))) : lr;
+        k_adam<<<grid_for(m->n_params), 256, 0, m->s>>>(m->p, m->m, m->v, m->g, m->n_params, lr_s, b1, b2, 1e-8f, c1,
+                                                        c2);
         mlp_sync_bf16(m);
-        cudaMemcpyAsync(&hist[s], m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->s);
+        cudaMemcpyAsync(dhist + s, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->s);
         g_launches += 3;
-        // the host copy of the batch indices must not be overwritten before its transfer
-        cudaStreamSynchronize(m->s);
     }
+    std::vector<float> hist(steps, 0.0f);
+    if (steps > 0) cudaMemcpyAsync(hist.data(), dhist, sizeof(float) * steps, cudaMemcpyDeviceToHost, m->s);
     if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
     if (loss_history)
         for (int s = 0; s < steps; ++s) loss_history[s] = hist[s];

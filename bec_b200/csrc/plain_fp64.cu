@@ -298,6 +298,18 @@ struct F_resid {
     }
 };
 
+// |a - prev|^2 and |a|^2: the fixed-point residual of the imaginary-time map between checks
+struct F_diff2 {
+    const double2 *a, *prev;
+    __device__ void operator()(int i, double *v) const
+    {
+        const double2 u = a[i], p = prev[i];
+        const double dx = u.x - p.x, dy = u.y - p.y;
+        v[0] = dx * dx + dy * dy;
+        v[1] = u.x * u.x + u.y * u.y;
+    }
+};
+
 inline int nblk(int n) { return (n + 255) / 256; }
 
 } // namespace
@@ -414,6 +426,12 @@ void plain_gs_residual(const double2 *ax, const double2 *hk, const GeomD &g, dou
                        cudaStream_t s)
 {
     reduce_sum<1>(F_resid{ax, hk, g, mu}, g.cells, out, tmp, s);
+    g_launches += 2;
+}
+
+void plain_diff2(const double2 *a, const double2 *prev, int n, double *out, double *tmp, cudaStream_t s)
+{
+    reduce_sum<2>(F_diff2{a, prev}, n, out, tmp, s);
     g_launches += 2;
 }
 

@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from ._abi import (BecDerived, BecGsOpts, BecGsReport, BecMoments, BecObs, BecParams, BecSchedule,
-                   BEC_GS_FIXED_STEPS, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
+                   BEC_GS_FIXED_STEPS, BEC_LR_CONSTANT, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbec.so")
@@ -55,8 +55,10 @@ SIGNATURES = {
     "bec_moments_device_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,
                                              C.c_void_p]),
     "bec_ground_state_coeffs": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32), _P(BecGsOpts), _dp, _dp,
-                                          _P(BecGsReport)]),
+                                          _P(C.c_float), _P(BecGsReport)]),
     "bec_warmstart_basis_size": (C.c_int32, []),
+    "bec_warmstart_set_basis": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                          _P(C.c_float)]),
     "bec_pulse_finite": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     "bec_render_projections": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_float), _P(C.c_float), _P(C.c_float),
                                          _P(C.c_float), _P(C.c_float), _P(C.c_float)]),
@@ -69,7 +71,7 @@ SIGNATURES = {
     "bec_mlp_gradients": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), C.c_int32, _P(C.c_float),
                                     _P(C.c_float)]),
     "bec_mlp_train": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), C.c_int32, C.c_int32, C.c_int32,
-                                C.c_float, C.c_uint64, _P(C.c_float)]),
+                                C.c_float, C.c_int32, C.c_uint64, _P(C.c_float)]),
 }
 
 
@@ -168,10 +170,10 @@ class Engine:
 
     # ---- ground state (calculateSteadyState, wigner.cu:84-175)
     def ground_state(self, group=0, mode=BEC_GS_FIXED_STEPS, max_steps=100, tol=1e-6, check_every=1,
-                     warm_start=None):
+                     warm_start=None, res_tol=0.0):
         d = self.derived[group]
         o = BecGsOpts()
-        o.mode, o.max_steps, o.check_every, o.tol = mode, max_steps, check_every, tol
+        o.mode, o.max_steps, o.check_every, o.tol, o.res_tol = mode, max_steps, check_every, tol, res_tol
         ws = None
         if warm_start is not None:
             ws = np.ascontiguousarray(warm_start, dtype=np.complex128).reshape(-1)
@@ -276,6 +278,42 @@ class Engine:
                     "bec_render_projections")
         return dict(xy_a=xy_a, xy_b=xy_b, zy_a=zy_a, zy_b=zy_b, levels_xy=lxy, levels_zy=lzy)
 
+    # ---- warm-start ground states (coefficients of the correction over Thomas-Fermi)
+    def ground_state_coeffs(self, groups=None, mode=BEC_GS_FIXED_STEPS, max_steps=100, tol=1e-6, check_every=20,
+                            res_tol=0.0, coef_in=None, want_coef=True, want_profiles=False):
+        """Batched FP32 ground states of groups sharing one grid; returns (coef n x 64 or None,
+        profiles n x cells float32 or None, reports)."""
+        groups = list(range(self.n_groups)) if groups is None else list(groups)
+        n = len(groups)
+        nb = int(lib().bec_warmstart_basis_size())
+        o = BecGsOpts()
+        o.mode, o.max_steps, o.check_every, o.tol, o.res_tol = mode, max_steps, check_every, tol, res_tol
+        idx = (C.c_int32 * n)(*groups)
+        cin = None
+        if coef_in is not None:
+            cin = np.ascontiguousarray(coef_in, dtype=np.float64).reshape(n, nb)
+        cout = np.zeros((n, nb)) if want_coef else None
+        prof = np.zeros((n, self.derived[groups[0]].cells), dtype=np.float32) if want_profiles else None
+        reps = (BecGsReport * n)()
+        self._check(lib().bec_ground_state_coeffs(self._h, n, idx, C.byref(o),
+                                                  _dptr(cin) if cin is not None else None,
+                                                  _dptr(cout) if cout is not None else None,
+                                                  prof.ctypes.data_as(_P(C.c_float)) if prof is not None else None,
+                                                  reps), "bec_ground_state_coeffs")
+        return cout, prof, list(reps)
+
+    def set_warmstart_basis(self, grid, basis):
+        """Installs basis rows (nb x cells float32, nb <= 64) for grid (nvx, nvy, nvz); None removes it."""
+        nx, ny, nz = grid
+        if basis is None:
+            self._check(lib().bec_warmstart_set_basis(self._h, nx, ny, nz, 0, None), "bec_warmstart_set_basis")
+            return
+        b = np.ascontiguousarray(basis, dtype=np.float32)
+        if b.ndim != 2 or b.shape[1] != nx * ny * nz:
+            raise ValueError("basis shape")
+        self._check(lib().bec_warmstart_set_basis(self._h, nx, ny, nz, b.shape[0], b.ctypes.data_as(_P(C.c_float))),
+                    "bec_warmstart_set_basis")
+
     def profile_steps(self, n_steps, max_classes=16):
         """Per grid class: dict(dims, traj, z_ms, plane_ms) mean device time per launch."""
         dims = (C.c_int32 * (3 * max_classes))()
@@ -355,11 +393,11 @@ class MLP:
                     "bec_mlp_gradients")
         return float(loss.value), g
 
-    def train(self, x, target, steps, batch=256, lr=1e-3, seed=0):
+    def train(self, x, target, steps, batch=256, lr=1e-3, seed=0, schedule=BEC_LR_CONSTANT):
         x = np.ascontiguousarray(x, dtype=np.float32)
         t = np.ascontiguousarray(target, dtype=np.float32)
         hist = np.zeros(max(steps, 1), dtype=np.float32)
-        self._check(lib().bec_mlp_train(self._h, _fptr(x), _fptr(t), x.shape[0], batch, steps, lr, seed,
+        self._check(lib().bec_mlp_train(self._h, _fptr(x), _fptr(t), x.shape[0], batch, steps, lr, schedule, seed,
                                         _fptr(hist)), "bec_mlp_train")
         return hist[:steps]
 

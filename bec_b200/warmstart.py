@@ -5,23 +5,29 @@ Pipeline, all on the GPU through the C ABI:
      warm-start workload: N ~ U[5000, 100000], fx = fy and fz each scaled by
      U[0.9, 1.1], a11, a12, a22 each scaled by U[0.98, 1.02], grid 32x32x256;
   2. compute their ground states with the batched FP32 imaginary-time loop
-     (mu stopping rule) and keep only the least-squares coefficients of the
-     64-term correction over Thomas-Fermi (bec_ground_state_coeffs);
+     (|d mu|/mu and fixed-point residual rule, BEC_GS_MU_RESIDUAL). In Thomas-Fermi
+     scaled coordinates every parameter set lives on the same grid, so the scaled
+     corrections |psi|/A - f_TF of a first batch give a basis by proper orthogonal
+     decomposition (the normalised mean plus the leading modes of the deviations,
+     method of snapshots); it is installed on the device
+     (bec_warmstart_set_basis) and every ground state is reduced to its 64
+     least-squares coefficients (bec_ground_state_coeffs);
   3. train the MLP 6 -> 256 -> 256 -> 256 -> 64 (BF16 tensor-core GEMMs, FP32
      accumulation, Adam) to map normalised parameters to normalised coefficients;
   4. on held-out parameter sets, run the ground-state loop from Thomas-Fermi
      (cold) and from the network's prediction (warm) with the same stopping rule,
-     and compare iterations and device seconds.
-The network only seeds the loop; the loop and its |d mu|/mu rule decide.
+     and compare iterations and device seconds (warm: synthesis and loop, plus the
+     network's inference time).
+The network only seeds the loop; the loop and its stopping rule decide.
 """
-import ctypes as C
 import time
 
 import numpy as np
 
-from ._abi import BEC_GS_MU, BecGsOpts, BecGsReport
+from ._abi import BEC_GS_MU_RESIDUAL
 from .configs import A11, A12, A22, FX, FY, FZ, rb87_params
-from .engine import BEC_PATH_FP32_BATCHED, MLP, Engine, lib
+from ._abi import BEC_LR_COSINE
+from .engine import BEC_PATH_FP32_BATCHED, MLP, Engine, derive, lib
 
 GRID = (32, 32, 256)
 WIDTHS = [6, 256, 256, 256, 64]
@@ -40,97 +46,176 @@ def sample_params(n, seed, grid=GRID):
     return out
 
 
-def features(params):
-    """Normalised network inputs in [-1, 1]: log N, fx, fz, a11, a12, a22."""
-    lo, hi = np.log(N_RANGE[0]), np.log(N_RANGE[1])
-    f = []
+def raw_features(params):
+    """Network inputs before normalisation: log mu_TF and log lambda (in Thomas-Fermi scaled
+    coordinates the ground state depends on the parameters only through these two), then
+    log N, fx, fz and a11. All follow from (N, trap frequencies, scattering lengths)."""
+    out = []
     for p in params:
-        f.append([2 * (np.log(p.N) - lo) / (hi - lo) - 1,
-                  (p.fx / FX - 1) / 0.1, (p.fz / FZ - 1) / 0.1,
-                  (p.a11 / A11 - 1) / 0.02, (p.a12 / A12 - 1) / 0.02, (p.a22 / A22 - 1) / 0.02])
-    return np.array(f, dtype=np.float32)
+        d = derive(p)
+        out.append([np.log(d.mu), np.log(d.lambda_), np.log(p.N), p.fx, p.fz, p.a11])
+    return np.array(out, dtype=np.float64)
 
 
-def ground_states(params, coef_in=None, tol=1e-6, check_every=20, max_steps=40000, chunk=512):
-    """Batched ground states; returns (coefficients n x 64, steps, converged, mu, residual, device seconds)."""
+def ground_states(params, coef_in=None, basis=None, tol=1e-6, res_tol=0.0, check_every=20, max_steps=40000,
+                  chunk=512, want_profiles=False, mode=BEC_GS_MU_RESIDUAL):
+    """Batched ground states of parameter sets sharing one grid, `chunk` per launch sequence, with
+    `basis` (rows x cells) installed for the grid when given. Returns a dict: coef (n x 64), steps,
+    converged, mu, residual, step_residual, seconds (device, summed over chunks), profiles."""
     nb = int(lib().bec_warmstart_basis_size())
     n = len(params)
-    coef = np.zeros((n, nb))
-    steps = np.zeros(n, dtype=np.int64)
-    conv = np.zeros(n, dtype=bool)
-    mu = np.zeros(n)
-    res = np.zeros(n)
-    seconds = 0.0
+    grid = (params[0].nvx, params[0].nvy, params[0].nvz)
+    out = dict(coef=np.zeros((n, nb)), steps=np.zeros(n, dtype=np.int64), converged=np.zeros(n, dtype=bool),
+               mu=np.zeros(n), residual=np.zeros(n), step_residual=np.zeros(n), seconds=0.0,
+               profiles=[] if want_profiles else None)
     for a in range(0, n, chunk):
         part = params[a:a + chunk]
         m = len(part)
         eng = Engine(part, path=BEC_PATH_FP32_BATCHED)
-        o = BecGsOpts()
-        o.mode, o.max_steps, o.check_every, o.tol = BEC_GS_MU, max_steps, check_every, tol
-        idx = (C.c_int32 * m)(*range(m))
-        cout = np.zeros((m, nb))
-        reps = (BecGsReport * m)()
-        cin = None
-        if coef_in is not None:
-            cin = np.ascontiguousarray(coef_in[a:a + m], dtype=np.float64)
-        st = lib().bec_ground_state_coeffs(eng._h, m, idx, C.byref(o),
-                                           cin.ctypes.data_as(C.POINTER(C.c_double)) if cin is not None else None,
-                                           cout.ctypes.data_as(C.POINTER(C.c_double)), reps)
-        eng._check(st, "bec_ground_state_coeffs")
-        coef[a:a + m] = cout
+        if basis is not None:
+            eng.set_warmstart_basis(grid, basis)
+        cin = None if coef_in is None else coef_in[a:a + m]
+        coef, prof, reps = eng.ground_state_coeffs(mode=mode, max_steps=max_steps, tol=tol, check_every=check_every,
+                                                   res_tol=res_tol, coef_in=cin, want_profiles=want_profiles)
+        out["coef"][a:a + m] = coef
+        if want_profiles:
+            out["profiles"].append(prof)
         for k, r in enumerate(reps):
-            steps[a + k], conv[a + k], mu[a + k], res[a + k] = r.steps, bool(r.converged), r.mu, r.residual
-        seconds += reps[0].seconds
+            out["steps"][a + k], out["converged"][a + k] = r.steps, bool(r.converged)
+            out["mu"][a + k], out["residual"][a + k], out["step_residual"][a + k] = r.mu, r.residual, r.step_residual
+        out["seconds"] += reps[0].seconds
         eng.close()
-    return coef, steps, conv, mu, res, seconds
+    if want_profiles:
+        out["profiles"] = np.concatenate(out["profiles"])
+    return out
+
+
+def pod_basis(profiles, nb=64, rel_floor=1e-12):
+    """Proper orthogonal decomposition (method of snapshots) of scaled corrections (n x cells):
+    row 0 the normalised mean, then up to nb - 1 orthonormal modes of the deviations from it,
+    leading first (modes with eigenvalue below rel_floor x the largest are dropped). Returns the
+    float32 rows and the singular values of the deviations."""
+    R = np.asarray(profiles, dtype=np.float64)
+    mean = R.mean(axis=0)
+    X = R - mean
+    w, U = np.linalg.eigh(X @ X.T)
+    order = np.argsort(w)[::-1]
+    w, U = w[order], U[:, order]
+    keep = [i for i in range(min(nb - 1, len(w))) if w[i] > rel_floor * w[0]]
+    modes = (U[:, keep].T @ X) / np.sqrt(w[keep])[:, None]
+    B = np.vstack([mean[None] / np.linalg.norm(mean), modes])
+    return B.astype(np.float32), np.sqrt(np.maximum(w, 0.0))
+
+
+def project(basis, profiles, nb=64):
+    """Least-squares coefficients (n x nb, zero beyond the basis rows) of profiles on basis rows."""
+    B = np.asarray(basis, dtype=np.float64)
+    G = B @ B.T
+    c = np.linalg.solve(G, B @ np.asarray(profiles, dtype=np.float64).T).T
+    out = np.zeros((c.shape[0], nb))
+    out[:, :c.shape[1]] = c
+    return out
 
 
 class WarmStart:
-    """Trained network plus the coefficient normalisation."""
+    """Trained network plus its input range and output normalisation."""
 
-    def __init__(self, net, mean, std):
-        self.net, self.mean, self.std = net, mean, std
+    def __init__(self, net, f_lo, f_hi, mean, scale):
+        self.net, self.f_lo, self.f_hi, self.mean, self.scale = net, f_lo, f_hi, mean, scale
+
+    def features(self, params):
+        """Inputs mapped to [-1, 1] over the training set's range."""
+        return (2.0 * (raw_features(params) - self.f_lo) / (self.f_hi - self.f_lo) - 1.0).astype(np.float32)
 
     def predict(self, params):
-        y = self.net.forward(features(params))
-        return y.astype(np.float64) * self.std + self.mean
+        y = self.net.forward(self.features(params))
+        return y.astype(np.float64) * self.scale + self.mean
 
 
-def train(params, coef, steps=3000, batch=256, lr=1e-3, seed=0):
+def train(params, coef, steps=12000, batch=256, lr=1e-3, seed=0):
+    """Fits the MLP to the coefficients. Targets are centred and divided by one common scale, so
+    the squared loss weighs each basis row by its share of the profile (the rows are near
+    orthonormal) instead of inflating rows that only carry rounding-level variation; the
+    learning rate follows a cosine decay."""
+    F = raw_features(params)
+    f_lo, f_hi = F.min(axis=0), F.max(axis=0)
+    f_hi = np.where(f_hi > f_lo, f_hi, f_lo + 1.0)
     mean = coef.mean(axis=0)
-    std = coef.std(axis=0) + 1e-6
+    scale = float(np.sqrt(((coef - mean) ** 2).mean())) or 1.0
     net = MLP(WIDTHS, seed=seed)
-    hist = net.train(features(params), ((coef - mean) / std).astype(np.float32), steps=steps, batch=batch, lr=lr,
-                     seed=seed)
-    return WarmStart(net, mean, std), hist
+    ws = WarmStart(net, f_lo, f_hi, mean, scale)
+    hist = net.train(ws.features(params), ((coef - mean) / scale).astype(np.float32), steps=steps, batch=batch, lr=lr,
+                     seed=seed, schedule=BEC_LR_COSINE)
+    return ws, hist
 
 
-def run(n_train=4096, n_eval=256, seed=3, train_steps=3000, tol=1e-6, check_every=20, log=print):
+def run(n_train=4096, n_eval=256, n_pod=512, seed=3, train_steps=12000, tol=1e-6, res_tol=0.0, check_every=20,
+        grid=GRID, log=print):
     """The full pipeline; returns a dict of measured results."""
     t0 = time.time()
-    tr = sample_params(n_train, seed)
-    ev = sample_params(n_eval, seed + 1)
-    c_tr, s_tr, conv_tr, _, _, sec_tr = ground_states(tr, tol=tol, check_every=check_every)
-    log(f"training ground states: {n_train}, converged {conv_tr.mean():.3f}, mean steps {s_tr.mean():.0f}, "
-        f"{sec_tr:.1f} device s")
+    tr = sample_params(n_train, seed, grid)
+    ev = sample_params(n_eval, seed + 1, grid)
+    kw = dict(tol=tol, res_tol=res_tol, check_every=check_every)
+    # training ground states: the first n_pod give the basis, the rest are projected on the device
+    first = ground_states(tr[:n_pod], want_profiles=True, **kw)
+    basis, sv = pod_basis(first["profiles"])
+    rest = ground_states(tr[n_pod:], basis=basis, **kw) if n_train > n_pod else None
+    c_tr = project(basis, first["profiles"])
+    steps_tr = first["steps"]
+    sec_tr = first["seconds"]
+    if rest is not None:
+        c_tr = np.concatenate([c_tr, rest["coef"]])
+        steps_tr = np.concatenate([steps_tr, rest["steps"]])
+        sec_tr += rest["seconds"]
+    log(f"training ground states: {n_train}, mean steps {steps_tr.mean():.0f}, {sec_tr:.1f} device s; "
+        f"basis rows {basis.shape[0]}, sv[1:6]/sv[0] {np.round(sv[1:6] / sv[0], 5).tolist()}")
     ws, hist = train(tr, c_tr, steps=train_steps)
     log(f"training loss {hist[:10].mean():.4f} -> {hist[-10:].mean():.5f}")
-    c_cold, s_cold, conv_cold, mu_cold, res_cold, sec_cold = ground_states(ev, tol=tol, check_every=check_every)
+    cold = ground_states(ev, basis=basis, **kw)
+    ti = time.time()
     pred = ws.predict(ev)
-    c_warm, s_warm, conv_warm, mu_warm, res_warm, sec_warm = ground_states(ev, coef_in=pred, tol=tol,
-                                                                         check_every=check_every)
-    rel_coef_err = np.linalg.norm(pred - c_cold) / np.linalg.norm(c_cold - ws.mean)
+    t_inf = time.time() - ti
+    warm = ground_states(ev, coef_in=pred, basis=basis, **kw)
+    rel_coef_err = np.linalg.norm(pred - cold["coef"]) / np.linalg.norm(cold["coef"] - ws.mean)
     out = {
-        "n_train": n_train, "n_eval": n_eval, "train_steps": train_steps,
+        "grid": list(grid), "n_train": n_train, "n_eval": n_eval, "n_pod": n_pod, "train_steps": train_steps,
+        "rule": f"|dmu|/mu < {tol} and fixed-point residual < {res_tol if res_tol > 0 else 10 * tol}, "
+                f"checked every {check_every} steps",
+        "basis_rows": int(basis.shape[0]),
         "train_loss_first": float(hist[:10].mean()), "train_loss_last": float(hist[-10:].mean()),
-        "cold_steps_mean": float(s_cold.mean()), "warm_steps_mean": float(s_warm.mean()),
-        "cold_seconds": sec_cold, "warm_seconds": sec_warm,
-        "speedup_steps": float(s_cold.mean() / max(s_warm.mean(), 1)),
-        "speedup_seconds": float(sec_cold / max(sec_warm, 1e-9)),
-        "cold_converged": float(conv_cold.mean()), "warm_converged": float(conv_warm.mean()),
-        "mu_rel_diff_max": float(np.max(np.abs(mu_warm - mu_cold) / mu_cold)),
-        "residual_warm_max": float(res_warm.max()), "residual_cold_max": float(res_cold.max()),
+        "cold_steps_mean": float(cold["steps"].mean()), "warm_steps_mean": float(warm["steps"].mean()),
+        "cold_steps_max": int(cold["steps"].max()), "warm_steps_max": int(warm["steps"].max()),
+        "cold_seconds": cold["seconds"], "warm_seconds": warm["seconds"], "inference_seconds": t_inf,
+        "speedup_steps": float(cold["steps"].mean() / max(warm["steps"].mean(), 1)),
+        "speedup_seconds": float(cold["seconds"] / max(warm["seconds"] + t_inf, 1e-9)),
+        "cold_converged": float(cold["converged"].mean()), "warm_converged": float(warm["converged"].mean()),
+        "mu_rel_diff_max": float(np.max(np.abs(warm["mu"] - cold["mu"]) / cold["mu"])),
+        "residual_warm_max": float(warm["residual"].max()), "residual_cold_max": float(cold["residual"].max()),
         "coef_rel_err": float(rel_coef_err), "wall_s": time.time() - t0,
     }
     log(out)
     return out
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the warm-start network and compare cold and warm ground states")
+    ap.add_argument("--n-train", type=int, default=4096)
+    ap.add_argument("--n-eval", type=int, default=256)
+    ap.add_argument("--n-pod", type=int, default=512)
+    ap.add_argument("--train-steps", type=int, default=12000)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--grid", default="32x32x256")
+    ap.add_argument("--out", default=None, help="write the result dict as JSON here")
+    a = ap.parse_args(argv)
+    grid = tuple(int(v) for v in a.grid.split("x"))
+    out = run(n_train=a.n_train, n_eval=a.n_eval, n_pod=a.n_pod, seed=a.seed, train_steps=a.train_steps, grid=grid,
+              log=lambda m: print(m, flush=True))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define BEC_ABI_VERSION 1
+#define BEC_ABI_VERSION 2
 
 typedef enum bec_status {
     BEC_OK = 0,
@@ -111,7 +111,13 @@ typedef struct bec_derived {
 enum {
     BEC_GS_FIXED_STEPS = 0,  /* exactly max_steps imaginary-time steps */
     BEC_GS_MU = 1,           /* stop when |d mu| / mu < tol between checks */
-    BEC_GS_REFERENCE_E = 2   /* the reference's |dE/E| < 1e-6 test on its energy integral (wigner.cu:148-156) */
+    BEC_GS_REFERENCE_E = 2,  /* the reference's |dE/E| < 1e-6 test on its energy integral (wigner.cu:148-156) */
+    BEC_GS_MU_RESIDUAL = 3   /* MU's test and, at the same check, the fixed-point residual
+                              *   || psi_n - psi_{n-c} || / (c dt mu || psi_n ||) < res_tol
+                              * of the imaginary-time map (c = check_every, dt and mu in the
+                              * scaled units of bec_derived): mu alone passes through an extremum
+                              * on its way from Thomas-Fermi, where |d mu| is small long before
+                              * the state has stopped changing */
 };
 
 typedef struct bec_gs_opts {
@@ -121,6 +127,7 @@ typedef struct bec_gs_opts {
     int32_t warm_per_group;  /* bec_ground_state_batch: 1 = warm_start holds one start per listed group, back to back */
     double tol;              /* relative tolerance for MU mode (REFERENCE_E uses 1e-6) */
     const double *warm_start;/* optional x-space start (interleaved complex, cells); NULL = Thomas-Fermi */
+    double res_tol;          /* MU_RESIDUAL: bound on the fixed-point residual (<= 0: 10 tol) */
 } bec_gs_opts;
 
 typedef struct bec_gs_report {
@@ -131,6 +138,7 @@ typedef struct bec_gs_report {
     double N;                /* norm after the last renormalisation */
     double residual;         /* || H psi - mu psi || / || psi || */
     double seconds;          /* device time of the loop */
+    double step_residual;    /* MU / MU_RESIDUAL: the fixed-point residual at the last check (0 before two checks) */
 } bec_gs_report;
 
 /*
@@ -198,16 +206,28 @@ bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups
                                   bec_gs_report *reports);
 
 /* Ground states of n groups that share one grid, run batched in FP32 on the device
- * (FIXED_STEPS or MU rules, batched path only), exchanging only coefficients of the
- * 64-term correction over Thomas-Fermi with the host (bec_warmstart_basis_size):
- *   coef_in  (n x 64, may be NULL): warm starts psi = A max(f_TF + sum c_k B_k, 0),
- *            synthesised on the device (NULL = Thomas-Fermi);
- *   coef_out (n x 64, may be NULL): least-squares projection of each result;
- *   reports  (n, may be NULL): steps, convergence, mu, energy, residual (FP64 on the device).
- * The basis and scaling are documented in bec_b200/csrc/warmstart.cu. */
+ * (FIXED_STEPS, MU or MU_RESIDUAL rules, batched path only), exchanging only coefficients
+ * of the 64-term correction over Thomas-Fermi with the host (bec_warmstart_basis_size):
+ *   coef_in     (n x 64, may be NULL): warm starts psi = A max(f_TF + sum c_k B_k, 0),
+ *               synthesised on the device (NULL = Thomas-Fermi);
+ *   coef_out    (n x 64, may be NULL): least-squares projection of each result;
+ *   profile_out (n x cells floats, may be NULL): each result's scaled correction
+ *               |psi| / A - f_TF on the grid (the data a basis is learned from);
+ *   reports     (n, may be NULL): steps, convergence, mu, energy, residual (FP64 on the device);
+ *               seconds covers the warm-start synthesis and the loop.
+ * B_k is the basis installed for the grid by bec_warmstart_set_basis, else the analytic
+ * one; the basis and scaling are documented in bec_b200/csrc/warmstart.cu. */
 bec_status bec_ground_state_coeffs(bec_ctx *ctx, int32_t n, const int32_t *groups, const bec_gs_opts *opts,
-                                   const double *coef_in, double *coef_out, bec_gs_report *reports);
+                                   const double *coef_in, double *coef_out, float *profile_out,
+                                   bec_gs_report *reports);
 int32_t bec_warmstart_basis_size(void);
+
+/* Installs nb (1..64) basis rows of nvx*nvy*nvz floats (grid index order, scaled units as
+ * profile_out) for that grid in this context; coefficients k >= nb are then zero. nb = 0 or
+ * basis = NULL removes it (back to the analytic basis). BEC_ERR_INVALID_ARG when the rows are
+ * linearly dependent. */
+bec_status bec_warmstart_set_basis(bec_ctx *ctx, int32_t nvx, int32_t nvy, int32_t nvz, int32_t nb,
+                                   const float *basis);
 
 /* ---- evolution -------------------------------------------------------- */
 
@@ -327,9 +347,14 @@ bec_status bec_mlp_forward(bec_mlp *m, const float *x, int32_t batch, float *y);
 /* loss = mean over the batch and outputs of (y - target)^2 and its gradient (host layout) */
 bec_status bec_mlp_gradients(bec_mlp *m, const float *x, const float *target, int32_t batch, float *loss,
                              float *grads);
+/* Learning-rate schedules of bec_mlp_train */
+enum {
+    BEC_LR_CONSTANT = 0,     /* lr at every step */
+    BEC_LR_COSINE = 1        /* lr (1 + cos(pi step / steps)) / 2 */
+};
 /* Adam (beta 0.9, 0.999) on seeded minibatches of n samples; loss_history[step] (may be NULL) */
 bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_t n, int32_t batch, int32_t steps,
-                         float lr, uint64_t seed, float *loss_history);
+                         float lr, int32_t schedule, uint64_t seed, float *loss_history);
 
 /* ---- moments without device allocation -------------------------------- */
 

@@ -403,6 +403,7 @@ int oracle_ground_state(const bec_params *p, const bec_gs_opts *opts, double *ps
     double *kprop = malloc(sizeof(double) * cells);
     cplx *a = malloc(sizeof(cplx) * cells), *tmp = malloc(sizeof(cplx) * cells);
     cplx *tmp2 = malloc(sizeof(cplx) * cells);
+    cplx *prev = calloc(cells, sizeof(cplx));          /* x-space state at the previous check */
     oracle_potential_table(&d, V); oracle_k2_table(&d, k2h);
     for (int i = 0; i < cells; i++) kprop[i] = exp(-d.dt_steady / 2.0 * k2h[i]);   /* :128-134 */
 
@@ -423,8 +424,10 @@ int oracle_ground_state(const bec_params *p, const bec_gs_opts *opts, double *ps
     for (int i = 0; i < cells; i++) a[i] *= 1.0 / cells;
 
     const int itmax = d.itmax;
-    double E = 0.0, mu_prev = 0.0, mu = 0.0;
-    int steps = 0, converged = 0;
+    double E = 0.0, mu_prev = 0.0, mu = 0.0, step_res = 0.0;
+    int steps = 0, converged = 0, checks = 0;
+    const int mu_rule = opts->mode == BEC_GS_MU || opts->mode == BEC_GS_MU_RESIDUAL;
+    const double res_tol = opts->res_tol > 0.0 ? opts->res_tol : 10.0 * opts->tol;
     const int maxs = opts->max_steps > 0 ? opts->max_steps : 1;
     const int check = opts->check_every > 0 ? opts->check_every : 1;
     while (steps < maxs) {
@@ -453,10 +456,22 @@ int oracle_ground_state(const bec_params *p, const bec_gs_opts *opts, double *ps
             double newE = reference_energy(a, tmp, &f, V, k2h, &d);        /* :148 */
             if (fabs((newE - E) / newE) < 0.000001) stop = 1;              /* :155 */
             E = newE;
-        } else if (opts->mode == BEC_GS_MU && (steps % check) == 0) {
+        } else if (mu_rule && (steps % check) == 0) {
             gs_measures(a, tmp, tmp2, &f, V, k2h, &d, &mu, NULL, NULL, NULL);
-            if (mu_prev != 0.0 && fabs((mu - mu_prev) / mu) < opts->tol) stop = 1;
+            /* fixed-point residual || psi_n - psi_{n-c} || / (c dt mu || psi_n ||) */
+            double dd = 0.0, nn = 0.0;
+            for (int i = 0; i < cells; i++) {
+                const cplx e = a[i] - prev[i];
+                dd += creal(e) * creal(e) + cimag(e) * cimag(e);
+                nn += creal(a[i]) * creal(a[i]) + cimag(a[i]) * cimag(a[i]);
+                prev[i] = a[i];
+            }
+            const double r = sqrt(dd / nn) / ((double)check * d.dt_steady * fabs(mu));
+            if (checks > 0) step_res = r;
+            const int mu_ok = mu_prev != 0.0 && fabs((mu - mu_prev) / mu) < opts->tol;
+            if (mu_ok && (opts->mode == BEC_GS_MU || (checks > 0 && r < res_tol))) stop = 1;
             mu_prev = mu;
+            ++checks;
         }
         fft3d_run(&f, a, +1);                                               /* :151-152 */
         for (int i = 0; i < cells; i++) a[i] *= 1.0 / cells;
@@ -468,9 +483,10 @@ int oracle_ground_state(const bec_params *p, const bec_gs_opts *opts, double *ps
         memset(rep, 0, sizeof(*rep));
         rep->steps = steps;
         rep->converged = converged;
+        rep->step_residual = step_res;
         gs_measures(a, tmp, tmp2, &f, V, k2h, &d, &rep->mu, &rep->energy, &rep->residual, &rep->N);
     }
-    free(V); free(k2h); free(kprop); free(a); free(tmp); free(tmp2); fft3d_free(&f);
+    free(V); free(k2h); free(kprop); free(a); free(tmp); free(tmp2); free(prev); fft3d_free(&f);
     return BEC_OK;
 }
 

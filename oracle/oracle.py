@@ -119,10 +119,11 @@ def potential_table(d):
     return out
 
 
-def ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=100, tol=1e-6, check_every=1, warm_start=None):
+def ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=100, tol=1e-6, check_every=1, warm_start=None,
+                 res_tol=0.0):
     d = derive(p)
     o = BecGsOpts()
-    o.mode, o.max_steps, o.check_every, o.tol = mode, max_steps, check_every, tol
+    o.mode, o.max_steps, o.check_every, o.tol, o.res_tol = mode, max_steps, check_every, tol, res_tol
     ws = None
     if warm_start is not None:
         ws = np.ascontiguousarray(warm_start, dtype=np.complex128)

