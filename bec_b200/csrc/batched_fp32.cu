@@ -148,13 +148,12 @@ __global__ void __launch_bounds__(kThreads) k_ppass(float4 *state, ClassGeom c, 
             float2 ao = cmul(xa, da), bo = cmul(xb, db);
             if (P.noise) {
                 const uint32_t cell = (uint32_t)((z0 + p) * plane + y * c.nx + x);
-                float r1[4], r2[4];
-                normals4<float>(seed, tl, step, cell, RNG_TAG_LOSS1, r1);
-                normals4<float>(seed, tl, step, cell, RNG_TAG_LOSS2, r2);
+                float r[6];
+                loss_normals6<float>(seed, tl, step, cell, r);
                 const float s = P.noise_amp;
-                const float2 w1 = make_float2(s * r1[0], s * r1[1]);
-                const float2 w2 = make_float2(s * r1[2], s * r1[3]);
-                const float2 w3 = make_float2(s * r2[0], s * r2[1]);
+                const float2 w1 = make_float2(s * r[0], s * r[1]);
+                const float2 w2 = make_float2(s * r[2], s * r[3]);
+                const float2 w3 = make_float2(s * r[4], s * r[5]);
                 const float2 ca2 = cconj(a0), cb2 = cconj(b0);
                 ao = cadd(ao, cadd(cmul(cscale(cmul(ca2, ca2), P.c1), w1), cmul(cscale(cb2, P.c2), w2)));
                 bo = cadd(bo, cadd(cmul(cscale(ca2, P.c2), w2), cmul(cscale(cb2, P.c3), w3)));

@@ -218,7 +218,7 @@ bec_status get_tw64(bec_ctx *ctx, int n, double2 **out)
     std::vector<double2> t = twiddles(n);
     double2 *d = nullptr;
     CKC(dalloc(ctx, &d, t.size()));
-    CKC(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpyAsync(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
     ctx->tw64[n] = d;
     *out = d;
     return BEC_OK;
@@ -233,7 +233,7 @@ bec_status get_tw32(bec_ctx *ctx, int n, float2 **out)
     for (size_t i = 0; i < t.size(); ++i) f[i] = make_float2((float)t[i].x, (float)t[i].y);
     float2 *d = nullptr;
     CKC(dalloc(ctx, &d, f.size()));
-    CKC(cudaMemcpy(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpyAsync(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
     ctx->tw32[n] = d;
     *out = d;
     return BEC_OK;
@@ -251,7 +251,7 @@ bec_status get_tw32_full(bec_ctx *ctx, int n, float2 **out)
     }
     float2 *d = nullptr;
     CKC(dalloc(ctx, &d, f.size()));
-    CKC(cudaMemcpy(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpyAsync(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
     ctx->tw32_full[n] = d;
     *out = d;
     return BEC_OK;
@@ -668,8 +668,8 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
     {
         std::vector<int> first(ng), count(ng);
         for (int g = 0; g < ng; ++g) { first[g] = ctx->groups[g].traj_first; count[g] = ctx->groups[g].p.ne; }
-        CKA(cudaMemcpy(ctx->d_group_first, first.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
-        CKA(cudaMemcpy(ctx->d_group_count, count.data(), sizeof(int) * ng, cudaMemcpyHostToDevice));
+        CKA(cudaMemcpyAsync(ctx->d_group_first, first.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
+        CKA(cudaMemcpyAsync(ctx->d_group_count, count.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
     }
     if (path == BEC_PATH_FP64_PLAIN) {
         for (auto &gr : ctx->groups) {
@@ -684,12 +684,12 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
         std::vector<GroupParamsF> gfs(ng);
         for (int g = 0; g < ng; ++g) gfs[g] = ctx->groups[g].gf;
         CKA(dalloc(ctx, &ctx->d_gparams, (size_t)ng));
-        CKA(cudaMemcpy(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice));
+        CKA(cudaMemcpyAsync(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice, ctx->stream));
         for (auto &c : ctx->classes) {
             const size_t nt = (size_t)c.geom.n_traj;
             c.tiles = fp32_zpass_tiles(c.geom);
             CKA(dalloc(ctx, &c.state, nt * c.geom.cells));
-            CKA(cudaMemset(c.state, 0, sizeof(float4) * nt * c.geom.cells));
+            CKA(cudaMemsetAsync(c.state, 0, sizeof(float4) * nt * c.geom.cells, ctx->stream));
             CKA(dalloc(ctx, &c.d_tgroup, nt));
             CKA(dalloc(ctx, &c.d_tlocal, nt));
             CKA(dalloc(ctx, &c.d_traj_scale, nt));
@@ -706,9 +706,9 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
                     ts[gr.local_first + t] = (double)c.geom.nx * c.geom.ny * gr.d.dV;
                 }
             }
-            CKA(cudaMemcpy(c.d_tgroup, tg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
-            CKA(cudaMemcpy(c.d_tlocal, tl.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
-            CKA(cudaMemcpy(c.d_traj_scale, ts.data(), sizeof(double) * nt, cudaMemcpyHostToDevice));
+            CKA(cudaMemcpyAsync(c.d_tgroup, tg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, ctx->stream));
+            CKA(cudaMemcpyAsync(c.d_tlocal, tl.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, ctx->stream));
+            CKA(cudaMemcpyAsync(c.d_traj_scale, ts.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, ctx->stream));
         }
         CKA(dalloc(ctx, &ctx->scratch4, (size_t)ctx->max_cells));
     }
@@ -1025,7 +1025,7 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
                     h[t * cells + i] = make_float2((float)opts->warm_start[2 * src], (float)opts->warm_start[2 * src + 1]);
                 }
             CKC(talloc((void **)&c.warm, sizeof(float2) * nt * cells));
-            CKC(cudaMemcpy(c.warm, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+            CKC(cudaMemcpyAsync(c.warm, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
         } else if (coef_in) {
             const int nb = warmstart_basis_size();
             std::vector<double> cc(nt * nb);
@@ -1349,7 +1349,7 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
             void *p = nullptr;
             CKC(cudaMalloc(&p, sizeof(float2) * h.size()));
             nz = (float2 *)p;
-            cudaError_t e = cudaMemcpy(nz, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+            cudaError_t e = cudaMemcpyAsync(nz, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream);
             if (e != cudaSuccess) { cudaFree(p); return fail(ctx, BEC_ERR_CUDA, cudaGetErrorString(e)); }
         }
         ClassRec &c = ctx->classes[gr.cls];

@@ -67,7 +67,49 @@ BEC_HD u32x4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, u
 }
 
 // Stream tags of the counter's fourth word.
-enum { RNG_TAG_INIT = 0, RNG_TAG_LOSS1 = 1, RNG_TAG_LOSS2 = 2 };
+enum { RNG_TAG_INIT = 0, RNG_TAG_LOSS = 1 };
+
+// The loss noise of one cell and step takes one Philox4x32-10 draw: its 128 bits are cut
+// into six 21-bit fields, read as three Box-Muller pairs (u1 = (f + 1/2) / 2^21 in (0, 1),
+// u2 = f / 2^21), i.e. six normals truncated beyond 5.5 standard deviations (tail mass 4e-8).
+__host__ __device__ __forceinline__ void loss_fields(u32x4 w, uint32_t f[6])
+{
+    f[0] = w.x & 0x1FFFFFu;
+    f[1] = (w.x >> 21) | ((w.y & 0x3FFu) << 11);
+    f[2] = (w.y >> 10) & 0x1FFFFFu;
+    f[3] = (w.y >> 31) | ((w.z & 0xFFFFFu) << 1);
+    f[4] = (w.z >> 20) | ((w.w & 0x1FFu) << 12);
+    f[5] = (w.w >> 9) & 0x1FFFFFu;
+}
+
+__device__ __forceinline__ void box_muller21(uint32_t f1, uint32_t f2, double &n1, double &n2)
+{
+    const double r = sqrt(-2.0 * log(((double)f1 + 0.5) * 0x1p-21));
+    double s, c;
+    sincospi(2.0 * ((double)f2 * 0x1p-21), &s, &c);
+    n1 = r * c;
+    n2 = r * s;
+}
+
+__device__ __forceinline__ void box_muller21(uint32_t f1, uint32_t f2, float &n1, float &n2)
+{
+    const float r = sqrtf(-2.0f * logf(((float)f1 + 0.5f) * 0x1p-21f));
+    float s, c;
+    sincospif(2.0f * ((float)f2 * 0x1p-21f), &s, &c);
+    n1 = r * c;
+    n2 = r * s;
+}
+
+// The six loss-noise normals of (seed, trajectory, step, cell).
+template <typename R>
+__device__ __forceinline__ void loss_normals6(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell, R out[6])
+{
+    uint32_t f[6];
+    loss_fields(philox4x32_10(cell, step, traj, RNG_TAG_LOSS, (uint32_t)seed, (uint32_t)(seed >> 32)), f);
+    box_muller21(f[0], f[1], out[0], out[1]);
+    box_muller21(f[2], f[3], out[2], out[3]);
+    box_muller21(f[4], f[5], out[4], out[5]);
+}
 
 // Box-Muller from two 32-bit words. u1 = (x1 + 1) / 2^32 in (0, 1],
 // u2 = x2 / 2^32; -ln(u1) is taken through log1p near u1 = 1 so both tails

@@ -110,6 +110,188 @@ __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, in
     for (int y = 0; y < N; ++y) g[y * N + c] = v[y];
 }
 
+// ---------------------------------------------------------------- plane pass, 32 x 32, two warps a plane
+// The same plane step for N = 32 with every 32-point line shared by lane L of warp 0 and lane L of
+// warp 1 of the plane's CTA (h = warp): each holds 16 elements, half the registers of k_plane<32>,
+// so more warps fit on an SM. Forward transforms are split by decimation in time: x[2j + h] in, a
+// local 16-point DFT, one exchange of 8 values through shared memory, X[k] out in the block layout
+// kblk(s, h) (h = 0: k = 0..7, 16..23; h = 1: k = 8..15, 24..31). Inverse transforms use decimation
+// in frequency through IFFT(v) = conj(FFT(conj v)): block layout in, x[2m + h] out, which is the
+// layout the next forward step expects. The 32 x 32 float4 tile is swizzled like k_plane's.
+namespace split32 {
+
+__device__ __forceinline__ int kblk(int s, int h) { return s < 8 ? s + 8 * h : s + 8 + 8 * h; }
+__device__ __forceinline__ int tix(int row, int col) { return row * 32 + (col ^ (row & 7)); }
+
+// v * e^{-2 pi i K / 32}
+template <int K>
+__device__ __forceinline__ float4 w32(float4 v)
+{
+    if constexpr (K == 0) {
+        return v;
+    } else if constexpr (K == 8) {
+        return fftreg::mul_negi(v);
+    } else {
+        constexpr float c = (float)fftreg::cos_2pi(K, 32), sn = (float)fftreg::sin_2pi(K, 32);
+        return fftreg::cmulc(v, c, -sn);
+    }
+}
+
+// decimation in time, after the local DFT16: H = 0 keeps Y0[I] and receives Y1[I] -> X[I], X[16 + I];
+// H = 1 keeps Y1[8 + I] and receives Y0[8 + I] -> X[8 + I], X[24 + I]
+template <int H, int I>
+__device__ __forceinline__ void dit_send_one(const float4 *v, float4 *xo) { xo[I * 32] = H == 0 ? v[8 + I] : v[I]; }
+template <int H, int I>
+__device__ __forceinline__ void dit_recv_one(float4 *v, const float4 *xi)
+{
+    const float4 r = xi[I * 32];
+    const float4 e = H == 0 ? v[I] : r;
+    const float4 t = w32<H == 0 ? I : 8 + I>(H == 0 ? r : v[8 + I]);
+    v[I] = fftreg::add(e, t);
+    v[8 + I] = fftreg::sub(e, t);
+}
+// decimation in frequency, before the local DFT16: n = I (H = 0) or 8 + I (H = 1),
+// a[n] = x[n] + x[n + 16], b[n] = (x[n] - x[n + 16]) W^n; H = 0 gathers a[0..15], H = 1 b[0..15]
+template <int H, int I>
+__device__ __forceinline__ void dif_send_one(float4 *v, float4 *xo)
+{
+    const float4 a = fftreg::add(v[I], v[8 + I]);
+    const float4 b = w32<H == 0 ? I : 8 + I>(fftreg::sub(v[I], v[8 + I]));
+    if constexpr (H == 0) {
+        v[I] = a;
+        xo[I * 32] = b;
+    } else {
+        v[8 + I] = b;
+        xo[I * 32] = a;
+    }
+}
+template <int H, int I>
+__device__ __forceinline__ void dif_recv_one(float4 *v, const float4 *xi)
+{
+    if constexpr (H == 0) v[8 + I] = xi[I * 32];
+    else v[I] = xi[I * 32];
+}
+
+template <int H, int... I>
+__device__ __forceinline__ void dit_send(const float4 *v, float4 *xo, std::integer_sequence<int, I...>) { (dit_send_one<H, I>(v, xo), ...); }
+template <int H, int... I>
+__device__ __forceinline__ void dit_recv(float4 *v, const float4 *xi, std::integer_sequence<int, I...>) { (dit_recv_one<H, I>(v, xi), ...); }
+template <int H, int... I>
+__device__ __forceinline__ void dif_send(float4 *v, float4 *xo, std::integer_sequence<int, I...>) { (dif_send_one<H, I>(v, xo), ...); }
+template <int H, int... I>
+__device__ __forceinline__ void dif_recv(float4 *v, const float4 *xi, std::integer_sequence<int, I...>) { (dif_recv_one<H, I>(v, xi), ...); }
+
+using Seq8 = std::make_integer_sequence<int, 8>;
+
+// forward: v[j] = x[2j + h] -> v[s] = X[kblk(s, h)]; xb: the plane's exchange slots [2][8][32]
+__device__ __forceinline__ void fwd_line(float4 *v, float4 *xb, int h, int lane)
+{
+    dft<16, false>(v);
+    float4 *xo = xb + h * 256 + lane;
+    const float4 *xi = xb + (1 - h) * 256 + lane;
+    if (h == 0) dit_send<0>(v, xo, Seq8{});
+    else dit_send<1>(v, xo, Seq8{});
+    __syncthreads();
+    if (h == 0) dit_recv<0>(v, xi, Seq8{});
+    else dit_recv<1>(v, xi, Seq8{});
+}
+
+// inverse (unnormalised): v[s] = x[kblk(s, h)] -> v[m] = y[2m + h]
+__device__ __forceinline__ void inv_line(float4 *v, float4 *xb, int h, int lane)
+{
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
+    float4 *xo = xb + h * 256 + lane;
+    const float4 *xi = xb + (1 - h) * 256 + lane;
+    if (h == 0) dif_send<0>(v, xo, Seq8{});
+    else dif_send<1>(v, xo, Seq8{});
+    __syncthreads();
+    if (h == 0) dif_recv<0>(v, xi, Seq8{});
+    else dif_recv<1>(v, xi, Seq8{});
+    dft<16, false>(v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
+}
+
+} // namespace split32
+
+template <int MINB>
+__global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ state, int nz, int cells,
+                                                      const GroupParamsF *__restrict__ gp,
+                                                      const int *__restrict__ tgroup, const int *__restrict__ tlocal,
+                                                      uint32_t step)
+{
+    using namespace split32;
+    __shared__ float4 tile[1024];
+    __shared__ float4 xb[512];
+    const int h = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int plane_id = blockIdx.x;
+    const int traj = plane_id / nz, z = plane_id - traj * nz;
+    float4 *__restrict__ g = state + (size_t)traj * cells + (size_t)z * 1024;
+    const GroupParamsF P = gp[tgroup[traj]];
+
+    float4 v[16];
+    // forward along y (lane = column), then along x (lane = row); shared code body
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = g[(2 * j + h) * 32 + lane];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = tile[tix(lane, 2 * j + h)];
+        }
+        fwd_line(v, xb, h, lane);
+        if (pass == 0) {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) tile[tix(kblk(s, h), lane)] = v[s];
+            __syncthreads();
+        }
+    }
+    // x-space: lane owns row y = lane, cells x = kblk(s, h); the physics runs as a rolled loop
+    // over those cells in the tile
+    {
+        const int r = lane;
+#pragma unroll
+        for (int s = 0; s < 16; ++s) tile[tix(r, kblk(s, h))] = v[s];
+        const float Y = -P.ymax + P.dy * (float)r;
+        const float Z = -P.zmax + P.dz * (float)z;
+        const float base = Y * Y + Z * Z * P.inv_lambda2;
+        const uint32_t tl = (uint32_t)tlocal[traj];
+        const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
+#pragma unroll 1
+        for (int s = 0; s < 16; ++s) {
+            const int x = kblk(s, h);
+            const float X = -P.xmax + P.dx * (float)x;
+            const float V = 0.5f * (X * X + base);
+            float4 *slot = tile + tix(r, x);
+            const float4 v0 = *slot;
+            float4 o = nonlinear_cell(v0, V, P);
+            if (P.noise) o = loss_noise_cell(o, v0, P, tl, step, cell0 + x);
+            *slot = o;
+        }
+#pragma unroll
+        for (int s = 0; s < 16; ++s) v[s] = tile[tix(r, kblk(s, h))];
+    }
+    __syncthreads();    // the partner's physics is done with the row, and its last exchange reads too
+    // inverse along x (lane = row), then along y (lane = column); shared code body
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) v[s] = tile[tix(kblk(s, h), lane)];
+        }
+        inv_line(v, xb, h, lane);
+        if (pass == 0) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) tile[tix(lane, 2 * m + h)] = v[m];
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 16; ++m) g[(2 * m + h) * 32 + lane] = v[m];
+}
+
 // ---------------------------------------------------------------- pencil pass
 struct PencilArgs {
     float frac;          // kick in units of dt (0.5 + 0.5 for a full step)
@@ -278,6 +460,14 @@ void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, con
     g_launches++;
 }
 
+template <int MINB>
+void launch_plane32s(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
+                     uint32_t step, cudaStream_t s)
+{
+    k_plane32s<MINB><<<c.n_traj * c.nz, 64, 0, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
+    g_launches++;
+}
+
 } // namespace
 
 bool fp32_fast_plane_supported(const ClassGeom &c)
@@ -299,7 +489,7 @@ void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, 
     switch (c.nx) {
     case 8: launch_plane<8>(state, c, gp, tgroup, tlocal, step, s); break;
     case 16: launch_plane<16>(state, c, gp, tgroup, tlocal, step, s); break;
-    case 32: launch_plane<32>(state, c, gp, tgroup, tlocal, step, s); break;
+    case 32: launch_plane32s<8>(state, c, gp, tgroup, tlocal, step, s); break;
     default: break;
     }
 }

@@ -351,9 +351,9 @@ bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed
         for (int o = 0; o < widths[l + 1]; ++o)
             for (int i = 0; i < widths[l]; ++i) h[m->woff[l] + (size_t)o * m->w[l] + i] = U(rng);
     }
-    cudaMemcpy(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
-    cudaMemset(m->m, 0, sizeof(float) * m->n_params);
-    cudaMemset(m->v, 0, sizeof(float) * m->n_params);
+    cudaMemcpyAsync(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, m->s);
+    cudaMemsetAsync(m->m, 0, sizeof(float) * m->n_params, m->s);
+    cudaMemsetAsync(m->v, 0, sizeof(float) * m->n_params, m->s);
     mlp_sync_bf16(m);
     if (cudaStreamSynchronize(m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);
     *out = m;
@@ -382,7 +382,8 @@ bec_status bec_mlp_get_params(bec_mlp *m, float *params)
 {
     if (!m || !params) return BEC_ERR_INVALID_ARG;
     std::vector<float> h(m->n_params);
-    if (cudaMemcpy(h.data(), m->p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return BEC_ERR_CUDA;
+    cudaMemcpyAsync(h.data(), m->p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, m->s);
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
     size_t k = 0;
     for (int l = 0; l < m->L; ++l) {
         for (int o = 0; o < m->w_real[l + 1]; ++o)
@@ -402,7 +403,7 @@ bec_status bec_mlp_set_params(bec_mlp *m, const float *params)
             for (int i = 0; i < m->w_real[l]; ++i) h[m->woff[l] + (size_t)o * m->w[l] + i] = params[k++];
         for (int o = 0; o < m->w_real[l + 1]; ++o) h[m->boff[l] + o] = params[k++];
     }
-    if (cudaMemcpy(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return BEC_ERR_CUDA;
+    if (cudaMemcpyAsync(m->p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, m->s) != cudaSuccess) return BEC_ERR_CUDA;
     mlp_sync_bf16(m);
     return cudaStreamSynchronize(m->s) == cudaSuccess ? BEC_OK : BEC_ERR_CUDA;
 }
@@ -488,8 +489,8 @@ bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_
             for (int c = 0; c < in_r; ++c) hx[(size_t)r * inw + c] = x[(size_t)r * in_r + c];
             for (int c = 0; c < out_r; ++c) ht[(size_t)r * ow + c] = target[(size_t)r * out_r + c];
         }
-        cudaMemcpy(dx, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice);
-        cudaMemcpy(dt, ht.data(), sizeof(float) * ht.size(), cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(dx, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice, m->s);
+        cudaMemcpyAsync(dt, ht.data(), sizeof(float) * ht.size(), cudaMemcpyHostToDevice, m->s);
     }
     // minibatches: consecutive slices of seeded shuffles of the n samples
     std::mt19937_64 rng(seed);
@@ -503,7 +504,7 @@ bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_
             if (pos >= n) { std::shuffle(order.begin(), order.end(), rng); pos = 0; }
             hidx[(size_t)s * rows + r] = order[pos++];
         }
-    if (steps > 0) cudaMemcpy(didx, hidx.data(), sizeof(int) * hidx.size(), cudaMemcpyHostToDevice);
+    if (steps > 0) cudaMemcpyAsync(didx, hidx.data(), sizeof(int) * hidx.size(), cudaMemcpyHostToDevice, m->s);
     const double pi = 3.14159265358979323846;
     for (int s = 0; s < steps; ++s) {
         const int *bidx = didx + (size_t)s * rows;

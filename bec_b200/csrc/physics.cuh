@@ -10,31 +10,32 @@
 // followed by the Wigner loss-noise increment at the start of the substep:
 //   a += 3 sqrt(l111/6) conj(a0)^2 dW1 + sqrt(l12/2) conj(b0) dW2
 //   b +=   sqrt(l12/2)  conj(a0)   dW2 + sqrt(l22)   conj(b0) dW3,
-// dW complex normal with <|dW|^2> = dt / dV, drawn from Philox4x32-10 keyed by
-// the ensemble seed with counter (cell, step, trajectory, channel tag).
+// dW complex normal with <|dW|^2> = dt / dV; the six normals of a cell and step
+// come from one Philox4x32-10 draw keyed by the ensemble seed with counter
+// (cell, step, trajectory, 1) (loss_normals6, common.cuh).
 #pragma once
 
 #include "common.cuh"
 #include "engine.h"
 
-// Box-Muller with the SFU log/sin/cos: ~1e-6 relative agreement with the
-// FP64 draws of the oracle for the same counter.
-__device__ __forceinline__ void box_muller_fast(uint32_t x1, uint32_t x2, float &n1, float &n2)
+// loss_normals6 with the SFU log/sin/cos
+__device__ __forceinline__ void box_muller21_fast(uint32_t f1, uint32_t f2, float &n1, float &n2)
 {
-    const float u1 = fmaf((float)x1, 0x1p-32f, 0x1p-32f);       // (x1 + 1) / 2^32 in (0, 1]
-    const float r = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f));
+    const float r = sqrtf(-2.0f * __logf(fmaf((float)f1, 0x1p-21f, 0x1p-22f)));
     float s, c;
-    __sincosf(6.28318530717958648f * ((float)x2 * 0x1p-32f), &s, &c);
+    __sincosf(6.28318530717958648f * ((float)f2 * 0x1p-21f), &s, &c);
     n1 = r * c;
     n2 = r * s;
 }
 
-__device__ __forceinline__ void normals4_fast(uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
-                                              uint32_t cell, uint32_t tag, float out[4])
+__device__ __forceinline__ void loss_normals6_fast(uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
+                                                   uint32_t cell, float out[6])
 {
-    const u32x4 r = philox4x32_10(cell, step, traj, tag, k0, k1);
-    box_muller_fast(r.x, r.y, out[0], out[1]);
-    box_muller_fast(r.z, r.w, out[2], out[3]);
+    uint32_t f[6];
+    loss_fields(philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1), f);
+    box_muller21_fast(f[0], f[1], out[0], out[1]);
+    box_muller21_fast(f[2], f[3], out[2], out[3]);
+    box_muller21_fast(f[4], f[5], out[4], out[5]);
 }
 
 // (cos t, sin t): Taylor series in t^2 for |t| <= 0.5 (truncation < 1.2e-11, below
@@ -90,13 +91,12 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupP
 __device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const GroupParamsF &P, uint32_t traj,
                                                   uint32_t step, uint32_t cell)
 {
-    float r1[4], r2[4];
-    normals4_fast(P.seed_lo, P.seed_hi, traj, step, cell, RNG_TAG_LOSS1, r1);
-    normals4_fast(P.seed_lo, P.seed_hi, traj, step, cell, RNG_TAG_LOSS2, r2);
+    float r[6];
+    loss_normals6_fast(P.seed_lo, P.seed_hi, traj, step, cell, r);
     const float s = P.noise_amp;
-    const float2 w1 = make_float2(s * r1[0], s * r1[1]);
-    const float2 w2 = make_float2(s * r1[2], s * r1[3]);
-    const float2 w3 = make_float2(s * r2[0], s * r2[1]);
+    const float2 w1 = make_float2(s * r[0], s * r[1]);
+    const float2 w2 = make_float2(s * r[2], s * r[3]);
+    const float2 w3 = make_float2(s * r[4], s * r[5]);
     const float2 ca = make_float2(v0.x, -v0.y), cb = make_float2(v0.z, -v0.w);
     const float2 da = cadd(cmul(cscale(cmul(ca, ca), P.c1), w1), cmul(cscale(cb, P.c2), w2));
     const float2 db = cadd(cmul(cscale(ca, P.c2), w2), cmul(cscale(cb, P.c3), w3));

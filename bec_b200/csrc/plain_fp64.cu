@@ -122,14 +122,13 @@ __global__ void k_nl(double2 *a, double2 *b, GeomD g, uint32_t traj, uint32_t st
     }
     double2 ao = cmul(x, da), bo = cmul(y, db);
     if (g.noise) {
-        double r1[4], r2[4];
-        normals4<double>(g.seed, traj, step, (uint32_t)i, RNG_TAG_LOSS1, r1);
-        normals4<double>(g.seed, traj, step, (uint32_t)i, RNG_TAG_LOSS2, r2);
+        double r[6];
+        loss_normals6<double>(g.seed, traj, step, (uint32_t)i, r);
         const double ns = sqrt(dt / (2.0 * g.dV));
         const double c1 = sqrt(g.l111 / 6.0) * 3.0, c2 = sqrt(g.l12 / 2.0), c3 = sqrt(g.l22);
-        double2 w1 = make_double2(ns * r1[0], ns * r1[1]);
-        double2 w2 = make_double2(ns * r1[2], ns * r1[3]);
-        double2 w3 = make_double2(ns * r2[0], ns * r2[1]);
+        double2 w1 = make_double2(ns * r[0], ns * r[1]);
+        double2 w2 = make_double2(ns * r[2], ns * r[3]);
+        double2 w3 = make_double2(ns * r[4], ns * r[5]);
         double2 ca = cconj(a0), cb = cconj(b0);
         ao = cadd(ao, cadd(cmul(cscale(cmul(ca, ca), c1), w1), cmul(cscale(cb, c2), w2)));
         bo = cadd(bo, cadd(cmul(cscale(ca, c2), w2), cmul(cscale(cb, c3), w3)));

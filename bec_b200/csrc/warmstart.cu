@@ -167,15 +167,17 @@ __global__ void k_ws_synth(float2 *psi, int n_traj, WsGeom g, const float *amp, 
 
 bool g_consts_set = false;
 
-cudaError_t set_consts()
+cudaError_t set_consts(cudaStream_t s)
 {
     if (g_consts_set) return cudaSuccess;
     float rc[kRad], rw[kRad];
     const float broad[4] = {0.0f, 0.3f, 0.55f, 0.75f};
     for (int a = 0; a < 4; ++a) { rc[a] = broad[a]; rw[a] = 0.22f; }
     for (int a = 4; a < kRad; ++a) { rc[a] = 0.80f + 0.045f * (a - 4); rw[a] = 0.06f; }
-    cudaError_t e = cudaMemcpyToSymbol(c_rc, rc, sizeof(rc));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rw, rw, sizeof(rw));
+    // stream-ordered (the work that reads them runs on s, which does not wait for the legacy stream)
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_rc, rc, sizeof(rc), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_rw, rw, sizeof(rw), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) g_consts_set = true;
     return e;
 }
@@ -277,7 +279,7 @@ cudaError_t warmstart_table_init(WsTable &t, const float *host_basis, cudaStream
 cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, const WsTable *tab, double *coef_out,
                               float *profile_out, cudaStream_t s)
 {
-    cudaError_t e = set_consts();
+    cudaError_t e = set_consts(s);
     if (e) return e;
     const WsGeom g = geom_dims(d[0].nvx, d[0].nvy, d[0].nvz);
     std::vector<float> amp(n);
@@ -320,7 +322,7 @@ cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, co
 cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, const WsTable *tab, float2 *psi_out,
                             cudaStream_t s)
 {
-    cudaError_t e = set_consts();
+    cudaError_t e = set_consts(s);
     if (e) return e;
     const WsGeom g = geom_dims(d[0].nvx, d[0].nvy, d[0].nvz);
     std::vector<float> amp(n), c((size_t)n * kBasis);

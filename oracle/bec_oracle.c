@@ -171,7 +171,30 @@ void oracle_normals4(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell,
     box_muller(r[2], r[3], &out[2], &out[3]);
 }
 
-enum { TAG_INIT = 0, TAG_LOSS1 = 1, TAG_LOSS2 = 2 };
+enum { TAG_INIT = 0, TAG_LOSS = 1 };
+
+/* The loss noise of one cell and step (builder definition; no reference counterpart):
+ * one Philox4x32-10 draw, counter (cell, step, traj, 1), its 128 bits cut into six 21-bit
+ * fields f0..f5 read as three Box-Muller pairs with u1 = (f + 1/2) / 2^21, u2 = f / 2^21. */
+void oracle_loss_normals6(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell, double out[6])
+{
+    uint32_t ctr[4] = {cell, step, traj, TAG_LOSS};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t w[4], f[6];
+    oracle_philox4x32_10(ctr, key, w);
+    f[0] = w[0] & 0x1FFFFFu;
+    f[1] = (w[0] >> 21) | ((w[1] & 0x3FFu) << 11);
+    f[2] = (w[1] >> 10) & 0x1FFFFFu;
+    f[3] = (w[1] >> 31) | ((w[2] & 0xFFFFFu) << 1);
+    f[4] = (w[2] >> 20) | ((w[3] & 0x1FFu) << 12);
+    f[5] = (w[3] >> 9) & 0x1FFFFFu;
+    for (int k = 0; k < 3; k++) {
+        double r = sqrt(-2.0 * log(((double)f[2 * k] + 0.5) * 0x1p-21));
+        double ang = 2.0 * M_PI * ((double)f[2 * k + 1] * 0x1p-21);
+        out[2 * k] = r * cos(ang);
+        out[2 * k + 1] = r * sin(ang);
+    }
+}
 
 /* ------------------------------------------------------------------ */
 /* FFT: iterative radix-2, unnormalised                                 */
@@ -605,12 +628,11 @@ static void step_traj(const oracle_ens *e, fft3d *f, cplx *a, cplx *b, int traj,
              *   db += sqrt(l12/2) conj(a) dW2 + sqrt(l22) conj(b) dW3
              * <dW dW*> = dt/dV per channel (diffusion of report.tex:700-720,
              * poster.tex:276-278 with kappa fixed by the drift of :208-215). */
-            double r1[4], r2[4];
-            oracle_normals4(e->p.seed, (uint32_t)traj, (uint32_t)step, (uint32_t)i, TAG_LOSS1, r1);
-            oracle_normals4(e->p.seed, (uint32_t)traj, (uint32_t)step, (uint32_t)i, TAG_LOSS2, r2);
-            cplx w1 = ns * (r1[0] + I * r1[1]);
-            cplx w2 = ns * (r1[2] + I * r1[3]);
-            cplx w3 = ns * (r2[0] + I * r2[1]);
+            double r[6];
+            oracle_loss_normals6(e->p.seed, (uint32_t)traj, (uint32_t)step, (uint32_t)i, r);
+            cplx w1 = ns * (r[0] + I * r[1]);
+            cplx w2 = ns * (r[2] + I * r[3]);
+            cplx w3 = ns * (r[4] + I * r[5]);
             cplx ca = conj(a0), cb = conj(b0);
             ao += c1 * ca * ca * w1 + c2 * cb * w2;
             bo += c2 * ca * w2 + c3 * cb * w3;

@@ -29,6 +29,8 @@ int oracle_derive(const bec_params *p, bec_derived *out);
 /* primitives exposed for known-answer tests */
 void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void oracle_normals4(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell, uint32_t tag, double out[4]);
+/* the six loss-noise normals of (seed, traj, step, cell): one Philox draw cut into 21-bit fields */
+void oracle_loss_normals6(uint64_t seed, uint32_t traj, uint32_t step, uint32_t cell, double out[6]);
 int oracle_fft3d(double *data, int nx, int ny, int nz, int sign);   /* unnormalised, sign -1 forward, +1 inverse */
 void oracle_k2_table(const bec_derived *d, double *k2half);          /* (kx^2+ky^2+kz^2)/2 per cell */
 void oracle_potential_table(const bec_derived *d, double *v);        /* V per cell */

@@ -39,6 +39,8 @@ def lib():
         L.oracle_philox4x32_10.restype = None
         L.oracle_normals4.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, dp]
         L.oracle_normals4.restype = None
+        L.oracle_loss_normals6.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, dp]
+        L.oracle_loss_normals6.restype = None
         L.oracle_fft3d.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.oracle_k2_table.argtypes = [P(BecDerived), dp]
         L.oracle_k2_table.restype = None
@@ -91,6 +93,12 @@ def philox(ctr, key):
     o = (C.c_uint32 * 4)()
     lib().oracle_philox4x32_10(c, k, o)
     return list(o)
+
+
+def loss_normals6(seed, traj, step, cell):
+    o = np.zeros(6)
+    lib().oracle_loss_normals6(seed, traj, step, cell, _dptr(o))
+    return o
 
 
 def normals4(seed, traj, step, cell, tag):

@@ -38,6 +38,27 @@ def test_normals_statistics():
     assert abs(((rng_vals - rng_vals.mean()) ** 4).mean() / rng_vals.var() ** 2 - 3.0) < 0.15
 
 
+def test_loss_normals_fields_and_statistics():
+    """Six normals per Philox draw: the 21-bit fields restated from the draw's words, and the
+    moments and mutual independence of the six outputs."""
+    seed, traj, step, cell = 0x1234567890AB, 3, 17, 4242
+    w = [int(v) for v in O.philox((cell, step, traj, 1), (seed & 0xFFFFFFFF, seed >> 32))]
+    bits = w[0] | (w[1] << 32) | (w[2] << 64) | (w[3] << 96)
+    f = [(bits >> (21 * k)) & 0x1FFFFF for k in range(6)]
+    expect = []
+    for k in range(3):
+        r = np.sqrt(-2.0 * np.log((f[2 * k] + 0.5) / 2.0 ** 21))
+        a = 2.0 * np.pi * f[2 * k + 1] / 2.0 ** 21
+        expect += [r * np.cos(a), r * np.sin(a)]
+    np.testing.assert_allclose(O.loss_normals6(seed, traj, step, cell), expect, rtol=1e-14, atol=1e-14)
+    v = np.array([O.loss_normals6(7, t, 3, c) for t in range(4) for c in range(5000)])
+    assert np.all(np.abs(v.mean(axis=0)) < 0.04)
+    assert np.all(np.abs(v.std(axis=0) - 1.0) < 0.03)
+    assert abs(((v - v.mean()) ** 4).mean() / v.var() ** 2 - 3.0) < 0.15
+    corr = np.corrcoef(v.T)
+    assert np.max(np.abs(corr - np.eye(6))) < 0.05
+
+
 # ---------------------------------------------------------------- FFT
 @pytest.mark.parametrize("shape", [(64, 8, 8), (128, 16, 16), (128, 1, 32), (16, 4, 2)])
 def test_fft_matches_numpy(shape):
