@@ -78,9 +78,10 @@ __global__ void k_init(float4 *state, int cells, int ne, GroupParamsF gp, const 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_ppass(float4 *state, ClassGeom c, int ppc, const GroupParamsF *gp,
                                                    const int *tgroup, const int *tlocal, const float2 *tw_x,
-                                                   const float2 *tw_y, uint32_t step)
+                                                   const float2 *tw_y, const uint32_t *stepp)
 {
     extern __shared__ float4 sm4[];
+    const uint32_t step = stepp ? *stepp : 0u;   // Philox step index (device scalar, see fp32_put_step)
     const int plane = c.nx * c.ny;
     const int chunk = ppc * plane;
     float4 *buf = sm4;
@@ -334,7 +335,7 @@ size_t ppass_smem(const ClassGeom &c, int ppc)
 
 template <int MODE>
 void launch_ppass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                  const float2 *tw_x, const float2 *tw_y, uint32_t step, cudaStream_t s)
+                  const float2 *tw_x, const float2 *tw_y, const uint32_t *step, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
     const int ppc = planes_per_cta(c);
@@ -360,18 +361,35 @@ void fp32_init_group(float4 *state, int cells, int ne, const GroupParamsF &gp, c
 
 void fp32_prep(float4 *state, const ClassGeom &c, const float2 *tw_x, const float2 *tw_y, cudaStream_t s)
 {
-    launch_ppass<1>(state, c, nullptr, nullptr, nullptr, tw_x, tw_y, 0, s);
+    launch_ppass<1>(state, c, nullptr, nullptr, nullptr, tw_x, tw_y, nullptr, s);
 }
 
 void fp32_unprep(float4 *state, const ClassGeom &c, const float2 *tw_x, const float2 *tw_y, cudaStream_t s)
 {
-    launch_ppass<2>(state, c, nullptr, nullptr, nullptr, tw_x, tw_y, 0, s);
+    launch_ppass<2>(state, c, nullptr, nullptr, nullptr, tw_x, tw_y, nullptr, s);
 }
 
 void fp32_ppass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                const float2 *tw_x, const float2 *tw_y, uint32_t step, cudaStream_t s)
+                const float2 *tw_x, const float2 *tw_y, const uint32_t *d_step, cudaStream_t s)
 {
-    launch_ppass<0>(state, c, gp, tgroup, tlocal, tw_x, tw_y, step, s);
+    launch_ppass<0>(state, c, gp, tgroup, tlocal, tw_x, tw_y, d_step, s);
+}
+
+namespace {
+__global__ void k_put_step(uint32_t *d, uint32_t v) { *d = v; }
+__global__ void k_inc_step(uint32_t *d) { *d += 1u; }
+} // namespace
+
+void fp32_put_step(uint32_t *d_step, uint32_t v, cudaStream_t s)
+{
+    k_put_step<<<1, 1, 0, s>>>(d_step, v);
+    g_launches++;
+}
+
+void fp32_inc_step(uint32_t *d_step, cudaStream_t s)
+{
+    k_inc_step<<<1, 1, 0, s>>>(d_step);
+    g_launches++;
 }
 
 int fp32_zpass_tiles(const ClassGeom &c)

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -72,6 +73,11 @@ struct bec_ctx {
     std::map<int, float2 *> tw32;
     std::map<int, float2 *> tw32_full;
     bool use_fast = true;                // register-resident passes where the shape allows
+    uint32_t *d_step = nullptr;          // batched: Philox step index the plane passes read
+    bool use_graphs = true;              // batched: steady steps replay captured CUDA graphs
+    bool graphs_failed = false;
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
+    long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
     GroupParamsF *d_gparams = nullptr;
     double *d_traj_tot = nullptr;        // [n_traj][4]
     double *d_group_mom = nullptr;       // [n_groups][4]
@@ -345,21 +351,25 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
     return BEC_OK;
 }
 
-bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr)
+// put_step: write ctx->step into the device step scalar first (eager launches); otherwise increment
+// it (the body of a captured step graph, replayed from a known start value)
+bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr, bool put_step = true)
 {
+    if (put_step) fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
+    else fp32_inc_step(ctx->d_step, ctx->stream);
+    CKL();
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
         const size_t ci = &c - &ctx->classes[0];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
         if (ctx->use_fast && fp32_fast_plane_supported(c.geom)) {
-            fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, (uint32_t)ctx->step, ctx->stream);
+            fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step, ctx->stream);
         } else {
             float2 *tx, *ty;
             bec_status st;
             if ((st = get_tw32(ctx, c.geom.nx, &tx))) return st;
             if ((st = get_tw32(ctx, c.geom.ny, &ty))) return st;
-            fp32_ppass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, tx, ty, (uint32_t)ctx->step,
-                       ctx->stream);
+            fp32_ppass(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, tx, ty, ctx->d_step, ctx->stream);
         }
         if (ev) CKC(cudaEventRecord(ev[ci].second, ctx->stream));
         CKL();
@@ -389,6 +399,82 @@ bec_status batched_resolve(bec_ctx *ctx, bool observe)
     bec_status st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.0f, observe, nullptr, true);
     if (st) return st;
     ctx->pending = false;
+    return BEC_OK;
+}
+
+// ---------------------------------------------------------------- captured step loop
+// A steady step (the previous step's second half-kick pending, no pulse, no observation) launches the
+// same kernels with the same arguments every time: the full kick in the pencil passes, an increment of
+// the device step scalar, the plane passes. kGraphSteps of them, and one, are captured once per context
+// and replayed; the device step scalar is set once before a stretch of replays.
+constexpr int kGraphSteps = 8;
+
+bec_status capture_steps(bec_ctx *ctx, int k, cudaGraphExec_t *out, long long *kernels)
+{
+    const long long l0 = g_launches;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return BEC_ERR_CUDA;
+    }
+    bec_status st = BEC_OK;
+    for (int i = 0; i < k && st == BEC_OK; ++i) {
+        st = batched_zpass_all(ctx, 0.5f, 0.5f, false, nullptr);
+        if (st == BEC_OK) st = batched_ppass_all(ctx, nullptr, false);
+    }
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    *kernels = g_launches - l0;
+    g_launches = l0;                    // captured, not launched
+    if (st != BEC_OK || e != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return st != BEC_OK ? st : BEC_ERR_CUDA;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        *out = nullptr;
+        cudaGetLastError();
+        return BEC_ERR_CUDA;
+    }
+    return BEC_OK;
+}
+
+// m steady steps (requires ctx->pending and no pulse waiting)
+bec_status run_steady(bec_ctx *ctx, long long m)
+{
+    if (m <= 0) return BEC_OK;
+    bool graphs = ctx->use_graphs && !ctx->graphs_failed;
+    if (graphs && !ctx->step_graph[0]) {
+        // every buffer and twiddle table a steady step touches exists once an eager step has run
+        if (capture_steps(ctx, kGraphSteps, &ctx->step_graph[0], &ctx->graph_kernels[0]) != BEC_OK ||
+            capture_steps(ctx, 1, &ctx->step_graph[1], &ctx->graph_kernels[1]) != BEC_OK) {
+            ctx->graphs_failed = true;
+            graphs = false;
+        }
+    }
+    if (!graphs) {
+        for (long long i = 0; i < m; ++i) {
+            bec_status st = batched_zpass_all(ctx, 0.5f, 0.5f, false, nullptr);
+            if (st) return st;
+            if ((st = batched_ppass_all(ctx))) return st;
+            ctx->step++;
+            ctx->evo_steps++;
+        }
+        return BEC_OK;
+    }
+    fp32_put_step(ctx->d_step, (uint32_t)(ctx->step - 1), ctx->stream);   // each replayed step increments first
+    CKL();
+    for (long long i = 0; i < m / kGraphSteps; ++i) {
+        CKC(cudaGraphLaunch(ctx->step_graph[0], ctx->stream));
+        g_launches += ctx->graph_kernels[0];
+    }
+    for (long long i = 0; i < m % kGraphSteps; ++i) {
+        CKC(cudaGraphLaunch(ctx->step_graph[1], ctx->stream));
+        g_launches += ctx->graph_kernels[1];
+    }
+    ctx->step += m;
+    ctx->evo_steps += m;
     return BEC_OK;
 }
 
@@ -441,13 +527,16 @@ bec_status do_evolve(bec_ctx *ctx, int n)
             ctx->evo_steps++;
         }
     } else {
-        for (int s = 0; s < n; ++s) {
+        int s = 0;
+        if (n > 0 && (!ctx->pending || ctx->has_pulse)) {      // an eager first step starts the stretch
             if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
             ctx->pending = true;
             if ((st = batched_ppass_all(ctx))) return st;
             ctx->step++;
             ctx->evo_steps++;
+            s = 1;
         }
+        if ((st = run_steady(ctx, n - s))) return st;
     }
     return BEC_OK;
 }
@@ -685,6 +774,11 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
         for (int g = 0; g < ng; ++g) gfs[g] = ctx->groups[g].gf;
         CKA(dalloc(ctx, &ctx->d_gparams, (size_t)ng));
         CKA(cudaMemcpyAsync(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice, ctx->stream));
+        CKA(dalloc(ctx, &ctx->d_step, (size_t)1));
+        {
+            const char *g = std::getenv("BEC_CUDA_GRAPHS");
+            ctx->use_graphs = !(g && g[0] == '0');
+        }
         for (auto &c : ctx->classes) {
             const size_t nt = (size_t)c.geom.n_traj;
             c.tiles = fp32_zpass_tiles(c.geom);
@@ -724,6 +818,8 @@ void bec_destroy(bec_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (void *p : ctx->allocs) cudaFree(p);
     for (auto &t : ctx->ws_tables) cudaFree(t.d_basis);
+    for (auto &g : ctx->step_graph)
+        if (g) cudaGraphExecDestroy(g);
     for (auto &gr : ctx->groups)
         if (gr.gs_dev) { /* owned through allocs */ }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1599,7 +1695,12 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
         }
     } else {
         bool obs_due = false;
-        for (int i = 1; i <= n; ++i) {
+        // before step j: a sample of the boundary after step j-1, or the pi pulse scheduled there
+        auto event_before = [&](int j) {
+            return ((j - 1) > 0 && (j - 1) % every == 0 && sample < n_samples) || j - 1 == sch->pi_pulse_step;
+        };
+        int i = 1;
+        while (i <= n) {
             if (obs_due) {
                 // observe the boundary after step i-1 with a pass that ends that step
                 if ((st = batched_resolve(ctx, true))) return st;
@@ -1609,12 +1710,20 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
             }
             // a pi pulse scheduled after step i-1 rides on this step's pencil pass (after any sample)
             if (i - 1 == sch->pi_pulse_step && (st = apply_pulse(ctx, pi_m))) return st;
-            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
-            ctx->pending = true;
-            if ((st = batched_ppass_all(ctx))) return st;
-            ctx->step++;
-            ctx->evo_steps++;
-            if (i % every == 0 && sample < n_samples) obs_due = true;
+            int len = 1;
+            if (ctx->pending && !ctx->has_pulse) {
+                // steady steps up to the next sample or pulse: captured graph replays
+                while (i + len <= n && !event_before(i + len)) ++len;
+                if ((st = run_steady(ctx, len))) return st;
+            } else {
+                if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
+                ctx->pending = true;
+                if ((st = batched_ppass_all(ctx))) return st;
+                ctx->step++;
+                ctx->evo_steps++;
+            }
+            i += len;
+            if ((i - 1) % every == 0 && sample < n_samples) obs_due = true;
         }
         if (obs_due) {
             if ((st = batched_resolve(ctx, true))) return st;
@@ -1837,6 +1946,12 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
 }
 
 int64_t bec_step_index(const bec_ctx *ctx) { return ctx ? ctx->step : -1; }
+
+int32_t bec_step_graphs(const bec_ctx *ctx)
+{
+    if (!ctx || !ctx->use_graphs || ctx->graphs_failed) return 0;
+    return (ctx->step_graph[0] ? 1 : 0) + (ctx->step_graph[1] ? 1 : 0);
+}
 double bec_last_device_ms(const bec_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
 int64_t bec_last_launch_count(const bec_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
 

@@ -103,7 +103,11 @@ void fp32_unprep(float4 *state, const ClassGeom &c, const float2 *tw_x, const fl
 void fp32_zpass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
                 const float2 *tw_z, const ZPassArgs &z, double *obs_partial, cudaStream_t s);
 void fp32_ppass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
-                const int *tlocal, const float2 *tw_x, const float2 *tw_y, uint32_t step, cudaStream_t s);
+                const int *tlocal, const float2 *tw_x, const float2 *tw_y, const uint32_t *d_step, cudaStream_t s);
+// the plane passes read the Philox step index from a device scalar, so a captured step graph can replay:
+// an eagerly launched step writes it (fp32_put_step), a graph step increments it (fp32_inc_step)
+void fp32_put_step(uint32_t *d_step, uint32_t v, cudaStream_t s);
+void fp32_inc_step(uint32_t *d_step, cudaStream_t s);
 int fp32_zpass_tiles(const ClassGeom &c);   // tiles per trajectory of the z pass (obs_partial layout)
 // obs_partial[traj][tile][z][4] -> traj_axial[traj][z][4] * traj_scale[traj] (1 if NULL),
 // traj_tot[traj][4] = sum over z; traj_axial may be NULL
@@ -167,7 +171,7 @@ extern thread_local long long g_launches;
 bool fp32_fast_plane_supported(const ClassGeom &c);
 bool fp32_fast_pencil_supported(const ClassGeom &c);
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     uint32_t step, cudaStream_t s);
+                     const uint32_t *d_step, cudaStream_t s);
 // tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times out_scale;
 // m: optional pulse matrix (row-major, 4 entries) or NULL; obs: when not NULL the pass
 // ends a step and writes per-z partial moments [traj][tile][z][4] (tiles = fp32_fast_pencil_tiles)

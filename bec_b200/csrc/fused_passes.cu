@@ -35,9 +35,10 @@ using fftreg::dft;
 template <int N>
 __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, int nz, int cells,
                                                const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
-                                               const int *__restrict__ tlocal, uint32_t step)
+                                               const int *__restrict__ tlocal, const uint32_t *__restrict__ stepp)
 {
     constexpr int W = 32 / N;          // planes per warp
+    const uint32_t step = *stepp;      // Philox step index (device scalar, see fp32_put_step)
     constexpr int PLANE = N * N;
     extern __shared__ float4 tile[];   // 4 warps x W planes x PLANE
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -219,9 +220,10 @@ template <int MINB>
 __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ state, int nz, int cells,
                                                       const GroupParamsF *__restrict__ gp,
                                                       const int *__restrict__ tgroup, const int *__restrict__ tlocal,
-                                                      uint32_t step)
+                                                      const uint32_t *__restrict__ stepp)
 {
     using namespace split32;
+    const uint32_t step = *stepp;
     __shared__ float4 tile[1024];
     __shared__ float4 xb[512];
     const int h = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -446,7 +448,7 @@ void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, co
 
 template <int N>
 void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                  uint32_t step, cudaStream_t s)
+                  const uint32_t *step, cudaStream_t s)
 {
     constexpr int W = 32 / N;
     const int planes = c.n_traj * c.nz;
@@ -462,7 +464,7 @@ void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, con
 
 template <int MINB>
 void launch_plane32s(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     uint32_t step, cudaStream_t s)
+                     const uint32_t *step, cudaStream_t s)
 {
     k_plane32s<MINB><<<c.n_traj * c.nz, 64, 0, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
     g_launches++;
@@ -483,7 +485,7 @@ bool fp32_fast_pencil_supported(const ClassGeom &c)
 }
 
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     uint32_t step, cudaStream_t s)
+                     const uint32_t *step, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
     switch (c.nx) {

@@ -48,6 +48,7 @@ SIGNATURES = {
     "bec_get_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "bec_set_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "bec_step_index": (C.c_int64, [C.c_void_p]),
+    "bec_step_graphs": (C.c_int32, [C.c_void_p]),
     "bec_last_device_ms": (C.c_double, [C.c_void_p]),
     "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
     "bec_profile_steps": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P(C.c_int32), _P(C.c_int64), _dp,
@@ -159,6 +160,10 @@ class Engine:
     @property
     def step_index(self):
         return int(lib().bec_step_index(self._h))
+
+    @property
+    def step_graphs(self):
+        return int(lib().bec_step_graphs(self._h))
 
     @property
     def last_device_ms(self):

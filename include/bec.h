@@ -307,6 +307,11 @@ bec_status bec_get_state(bec_ctx *ctx, int32_t group, int32_t traj, double *ab_o
 bec_status bec_set_state(bec_ctx *ctx, int32_t group, int32_t traj, const double *ab_in);
 int64_t bec_step_index(const bec_ctx *ctx);
 
+/* Batched path: steady steps (no pulse or sample due) replay CUDA graphs captured once per context
+ * (8 steps and 1 step; set BEC_CUDA_GRAPHS=0 in the environment before bec_create to launch them one by
+ * one instead). Returns the number of step graphs captured and in use (0 or 2). */
+int32_t bec_step_graphs(const bec_ctx *ctx);
+
 /* ---- timing ----------------------------------------------------------- */
 
 /* Device time of the last bec_evolve / bec_run call, milliseconds (CUDA events). */

@@ -202,6 +202,36 @@ def test_run_with_pi_pulse_and_axial(path):
     assert obs["visibility_scan"] == pytest.approx(eo.ref_visibility(), abs=1e-9 if path == BEC_PATH_FP64_PLAIN else FP32_VIS)
 
 
+def test_step_graphs_replay_bit_identical(monkeypatch):
+    """Steady steps replayed from captured CUDA graphs give the same bits as launching every kernel
+    (mixed grids, a 2D slice on the generic plane pass, samples, a pi pulse, then plain evolution)."""
+    groups = [
+        rb87_params(N=15000, grid=(8, 8, 64), ne=2, noise=True, seed=1),
+        rb87_params(N=40000, grid=(16, 16, 128), ne=1, noise=True, seed=2),
+        rb87_params(N=25000, grid=(32, 1, 128), ne=2, noise=True, seed=3),
+    ]
+    gss = [O.ground_state(copy_params(p, ne=1), max_steps=100)[0] for p in groups]
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("BEC_CUDA_GRAPHS", flag)
+        eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
+        for g, gs in enumerate(gss):
+            eng.init_group(g, gs)
+        eng.start_evolution()
+        mom = eng.run(100, sample_every=25, pi_pulse_step=50)
+        eng.evolve(37)
+        out[flag] = (mom, eng.moments(), [eng.get_state(g, t) for g, p in enumerate(groups) for t in range(p.ne)],
+                     eng.step_graphs, eng.step_index)
+        eng.close()
+    on, off = out["1"], out["0"]
+    assert on[3] == 2 and off[3] == 0
+    assert on[4] == off[4] >= 137
+    np.testing.assert_array_equal(on[0], off[0])
+    np.testing.assert_array_equal(on[1], off[1])
+    for a, b in zip(on[2], off[2]):
+        np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("path", PATHS)
 def test_evolve_and_run_agree(path):
     p = rb87_params(N=30000, grid=(8, 8, 64), ne=1, noise=True, seed=3)
