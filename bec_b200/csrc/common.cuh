@@ -66,6 +66,28 @@ BEC_HD u32x4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, u
     return u32x4{c0, c1, c2, c3};
 }
 
+// Two Philox4x32-10 draws under one key, their rounds interleaved: the two multiply chains are
+// independent, so each hides the other's latency, and the key schedule is computed once.
+struct u32x4x2 { u32x4 a, b; };
+
+__device__ __forceinline__ u32x4x2 philox4x32_10_x2(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                    uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
+                                                    uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t la0 = 0xD2511F53u * a0, ha0 = __umulhi(0xD2511F53u, a0);
+        const uint32_t la1 = 0xCD9E8D57u * a2, ha1 = __umulhi(0xCD9E8D57u, a2);
+        const uint32_t lb0 = 0xD2511F53u * b0, hb0 = __umulhi(0xD2511F53u, b0);
+        const uint32_t lb1 = 0xCD9E8D57u * b2, hb1 = __umulhi(0xCD9E8D57u, b2);
+        a0 = ha1 ^ a1 ^ k0; a2 = ha0 ^ a3 ^ k1; a1 = la1; a3 = la0;
+        b0 = hb1 ^ b1 ^ k0; b2 = hb0 ^ b3 ^ k1; b1 = lb1; b3 = lb0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return u32x4x2{u32x4{a0, a1, a2, a3}, u32x4{b0, b1, b2, b3}};
+}
+
 // Stream tags of the counter's fourth word.
 enum { RNG_TAG_INIT = 0, RNG_TAG_LOSS = 1 };
 

@@ -18,24 +18,16 @@
 #include "common.cuh"
 #include "engine.h"
 
-// loss_normals6 with the SFU log/sin/cos
-__device__ __forceinline__ void box_muller21_fast(uint32_t f1, uint32_t f2, float &n1, float &n2)
+// One Box-Muller pair of loss_normals6 scaled by amp, with the SFU log2/rsqrt/sin/cos:
+// r = amp sqrt(-2 ln u1), u1 = (f1 + 1/2) / 2^21 in (0, 1) so -2 ln u1 > 0 and the square root
+// is taken as y rsqrt(y); (n1, n2) = r (cos, sin)(2 pi f2 / 2^21).
+__device__ __forceinline__ float2 box_muller21_scaled(uint32_t f1, uint32_t f2, float amp)
 {
-    const float r = sqrtf(-2.0f * __logf(fmaf((float)f1, 0x1p-21f, 0x1p-22f)));
+    const float y = -1.38629436112f * __log2f(fmaf((float)f1, 0x1p-21f, 0x1p-22f));
+    const float r = amp * (y * rsqrtf(y));
     float s, c;
-    __sincosf(6.28318530717958648f * ((float)f2 * 0x1p-21f), &s, &c);
-    n1 = r * c;
-    n2 = r * s;
-}
-
-__device__ __forceinline__ void loss_normals6_fast(uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
-                                                   uint32_t cell, float out[6])
-{
-    uint32_t f[6];
-    loss_fields(philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1), f);
-    box_muller21_fast(f[0], f[1], out[0], out[1]);
-    box_muller21_fast(f[2], f[3], out[2], out[3]);
-    box_muller21_fast(f[4], f[5], out[4], out[5]);
+    __sincosf((float)f2 * (6.28318530717958648f * 0x1p-21f), &s, &c);
+    return make_float2(r * c, r * s);
 }
 
 // (cos t, sin t): Taylor series in t^2 for |t| <= 0.5 (truncation < 1.2e-11, below
@@ -87,18 +79,41 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupP
     return make_float4(ao.x, ao.y, bo.x, bo.y);
 }
 
-// Adds the loss-noise increment evaluated at v0 to out.
-__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const GroupParamsF &P, uint32_t traj,
-                                                  uint32_t step, uint32_t cell)
+// Loss-noise amplitudes of a trajectory: noise_amp x (c1, c2, c3), computed once per thread.
+struct LossAmps { float w1, w2, w3; };
+__device__ __forceinline__ LossAmps loss_amps(const GroupParamsF &P)
 {
-    float r[6];
-    loss_normals6_fast(P.seed_lo, P.seed_hi, traj, step, cell, r);
-    const float s = P.noise_amp;
-    const float2 w1 = make_float2(s * r[0], s * r[1]);
-    const float2 w2 = make_float2(s * r[2], s * r[3]);
-    const float2 w3 = make_float2(s * r[4], s * r[5]);
+    return LossAmps{P.noise_amp * P.c1, P.noise_amp * P.c2, P.noise_amp * P.c3};
+}
+
+// The increment of loss_noise_cell from a given Philox output.
+__device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const LossAmps &A, u32x4 w)
+{
+    uint32_t f[6];
+    loss_fields(w, f);
+    const float2 w1 = box_muller21_scaled(f[0], f[1], A.w1);
+    const float2 w2 = box_muller21_scaled(f[2], f[3], A.w2);
+    const float2 w3 = box_muller21_scaled(f[4], f[5], A.w3);
     const float2 ca = make_float2(v0.x, -v0.y), cb = make_float2(v0.z, -v0.w);
-    const float2 da = cadd(cmul(cscale(cmul(ca, ca), P.c1), w1), cmul(cscale(cb, P.c2), w2));
-    const float2 db = cadd(cmul(cscale(ca, P.c2), w2), cmul(cscale(cb, P.c3), w3));
+    const float2 da = cadd(cmul(cmul(ca, ca), w1), cmul(cb, w2));
+    const float2 db = cadd(cmul(ca, w2), cmul(cb, w3));
     return make_float4(out.x + da.x, out.y + da.y, out.z + db.x, out.w + db.y);
+}
+
+// loss_noise_cell for two cells of the same trajectory and step (interleaved Philox draws).
+__device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4 &out1, float4 v1, const LossAmps &A,
+                                                 uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
+                                                 uint32_t cell0, uint32_t cell1)
+{
+    const u32x4x2 w = philox4x32_10_x2(cell0, step, traj, RNG_TAG_LOSS, cell1, step, traj, RNG_TAG_LOSS, k0, k1);
+    out0 = loss_noise_apply(out0, v0, A, w.a);
+    out1 = loss_noise_apply(out1, v1, A, w.b);
+}
+
+// Adds the loss-noise increment evaluated at v0 to out: the six normals of one Philox4x32-10 draw
+// (loss_fields) as three complex Wiener increments w1, w2, w3 already scaled by their amplitudes.
+__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const LossAmps &A, uint32_t k0,
+                                                  uint32_t k1, uint32_t traj, uint32_t step, uint32_t cell)
+{
+    return loss_noise_apply(out, v0, A, philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1));
 }
