@@ -3,7 +3,7 @@
 // A thread holds a whole line (N <= 32 elements) in registers; the DFT is a
 // fully unrolled radix-2 Cooley-Tukey recursion whose twiddles are
 // compile-time constants, so trivial twiddles (1, -i, +i) cost nothing and
-// the rest become FMA immediates. Elements are float2 (one complex value) or
+// the rest become FMA immediates of six-FMA butterflies (bfly_w). Elements are float2 (one complex value) or
 // float4 (the two components a, b of one cell, transformed together).
 //
 // Twiddle values come from cos_2pi / sin_2pi below: exact octant reduction on the
@@ -89,6 +89,43 @@ __device__ __forceinline__ float4 cmulw(float4 v, float2 w)
     return make_float4(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x, v.z * w.x - v.w * w.y, v.z * w.y + v.w * w.x);
 }
 
+// ---- butterfly with a constant twiddle -------------------------------------------
+// x0 = e + w o, x1 = e - w o for the compile-time twiddle w = c + i s, in six FMAs per complex value
+// (Linzer and Feig, "Implementation of efficient FFT algorithms on fused multiply-add architectures",
+// IEEE Trans. Signal Processing 41, 1993): the larger of |c|, |s| is factored out, so with r = s / c
+// (or c / s) of magnitude <= 1, w o = c (o.re - r o.im, o.im + r o.re) (or s (r o.re - o.im, o.re + r o.im)),
+// and both outputs are one FMA each from e.
+__device__ __forceinline__ void bfly_c(float2 &x0, float2 &x1, float2 e, float2 o, float f, float r)
+{
+    const float ur = fmaf(-r, o.y, o.x), ui = fmaf(r, o.x, o.y);
+    x0 = make_float2(fmaf(f, ur, e.x), fmaf(f, ui, e.y));
+    x1 = make_float2(fmaf(-f, ur, e.x), fmaf(-f, ui, e.y));
+}
+__device__ __forceinline__ void bfly_s(float2 &x0, float2 &x1, float2 e, float2 o, float f, float r)
+{
+    const float ur = fmaf(r, o.x, -o.y), ui = fmaf(r, o.y, o.x);
+    x0 = make_float2(fmaf(f, ur, e.x), fmaf(f, ui, e.y));
+    x1 = make_float2(fmaf(-f, ur, e.x), fmaf(-f, ui, e.y));
+}
+
+// the butterfly of twiddle w = e^{-+2 pi i K / N} (sign - forward, + when INV)
+template <int K, int N, bool INV>
+__device__ __forceinline__ void bfly_w(float2 &x0, float2 &x1, float2 e, float2 o)
+{
+    constexpr double c = cos_2pi(K, N), s = INV ? sin_2pi(K, N) : -sin_2pi(K, N);
+    if constexpr ((c < 0 ? -c : c) >= (s < 0 ? -s : s)) bfly_c(x0, x1, e, o, (float)c, (float)(s / c));
+    else bfly_s(x0, x1, e, o, (float)s, (float)(c / s));
+}
+template <int K, int N, bool INV>
+__device__ __forceinline__ void bfly_w(float4 &x0, float4 &x1, float4 e, float4 o)
+{
+    float2 a0, a1, b0, b1;
+    bfly_w<K, N, INV>(a0, a1, make_float2(e.x, e.y), make_float2(o.x, o.y));
+    bfly_w<K, N, INV>(b0, b1, make_float2(e.z, e.w), make_float2(o.z, o.w));
+    x0 = make_float4(a0.x, a0.y, b0.x, b0.y);
+    x1 = make_float4(a1.x, a1.y, b1.x, b1.y);
+}
+
 // ---- DFT ---------------------------------------------------------------------
 // x[k] <- sum_n x[n] exp(-+2 pi i n k / N) (sign - forward, + when INV), unnormalised.
 template <int N, bool INV, typename T>
@@ -97,18 +134,13 @@ __device__ __forceinline__ void dft(T *x);
 template <int N, bool INV, int K, typename T>
 __device__ __forceinline__ void combine_one(T *x, const T *e, const T *o)
 {
-    T t;
-    if constexpr (K == 0) {
-        t = o[K];
-    } else if constexpr (4 * K == N) {
-        t = INV ? mul_posi(o[K]) : mul_negi(o[K]);
+    if constexpr (K == 0 || 4 * K == N) {
+        const T t = K == 0 ? o[K] : INV ? mul_posi(o[K]) : mul_negi(o[K]);
+        x[K] = add(e[K], t);
+        x[K + N / 2] = sub(e[K], t);
     } else {
-        constexpr double c = cos_2pi(K, N);
-        constexpr double s = sin_2pi(K, N);
-        t = cmulc(o[K], (float)c, INV ? (float)s : -(float)s);
+        bfly_w<K, N, INV>(x[K], x[K + N / 2], e[K], o[K]);
     }
-    x[K] = add(e[K], t);
-    x[K + N / 2] = sub(e[K], t);
 }
 
 template <int N, bool INV, typename T, int... K>

@@ -151,9 +151,15 @@ __device__ __forceinline__ void dit_recv_one(float4 *v, const float4 *xi)
 {
     const float4 r = xi[I * 32];
     const float4 e = H == 0 ? v[I] : r;
-    const float4 t = w32<H == 0 ? I : 8 + I>(H == 0 ? r : v[8 + I]);
-    v[I] = fftreg::add(e, t);
-    v[8 + I] = fftreg::sub(e, t);
+    const float4 o = H == 0 ? r : v[8 + I];
+    constexpr int K = H == 0 ? I : 8 + I;
+    if constexpr (K == 0 || K == 8) {
+        const float4 t = w32<K>(o);
+        v[I] = fftreg::add(e, t);
+        v[8 + I] = fftreg::sub(e, t);
+    } else {
+        fftreg::bfly_w<K, 32, false>(v[I], v[8 + I], e, o);
+    }
 }
 // decimation in frequency, before the local DFT16: n = I (H = 0) or 8 + I (H = 1),
 // a[n] = x[n] + x[n + 16], b[n] = (x[n] - x[n + 16]) W^n; H = 0 gathers a[0..15], H = 1 b[0..15]

@@ -30,30 +30,21 @@ __device__ __forceinline__ float2 box_muller21_scaled(uint32_t f1, uint32_t f2, 
     return make_float2(r * c, r * s);
 }
 
-// (cos t, sin t): Taylor series in t^2 for |t| <= 0.5 (truncation < 1.2e-11, below
-// FP32 rounding), sincosf beyond.
-__device__ __forceinline__ float2 cis_small(float t)
+// Phase and decay factors of the nonlinear substep. On the bench workloads |t| = |Im p| dt/2 stays below
+// 0.38 and |Re p| dt/2 below 1e-6, so every cell takes the polynomial branch:
+//   cos t, sin t: Taylor in u = t^2, Horner form, for |t| <= 0.5; sin to t^7 (truncation <= 0.5^9/9! = 5.4e-9),
+//     cos to t^8 (<= 0.5^10/10! = 2.7e-10), both below half an FP32 ulp of the result;
+//   exp x: Taylor to x^3 for |x| <= 1/64 (truncation <= (1/64)^4/4! = 2.5e-9).
+// Arguments outside those ranges take sincosf / expf; one branch covers all four arguments of a cell.
+__device__ __forceinline__ float2 cis_taylor(float t)
 {
-    if (fabsf(t) <= 0.5f) {
-        const float u = t * t;
-        const float s = t * (1.f - u * (1.f / 6.f) * (1.f - u * (1.f / 20.f) * (1.f - u * (1.f / 42.f) *
-                                                                                    (1.f - u * (1.f / 72.f)))));
-        const float c = 1.f - u * 0.5f * (1.f - u * (1.f / 12.f) * (1.f - u * (1.f / 30.f) *
-                                                                   (1.f - u * (1.f / 56.f) * (1.f - u * (1.f / 90.f)))));
-        return make_float2(c, s);
-    }
-    float s, c;
-    sincosf(t, &s, &c);
+    const float u = t * t;
+    const float s = fmaf(t * u, fmaf(u, fmaf(u, -1.f / 5040.f, 1.f / 120.f), -1.f / 6.f), t);
+    const float c = fmaf(u, fmaf(u, fmaf(u, fmaf(u, 1.f / 40320.f, -1.f / 720.f), 1.f / 24.f), -0.5f), 1.f);
     return make_float2(c, s);
 }
 
-// exp(x): Taylor series for |x| <= 1/64 (truncation < 1e-11), expf beyond.
-__device__ __forceinline__ float exp_small(float x)
-{
-    if (fabsf(x) <= 0.015625f)
-        return 1.f + x * (1.f + x * 0.5f * (1.f + x * (1.f / 3.f) * (1.f + x * 0.25f * (1.f + x * 0.2f))));
-    return expf(x);
-}
+__device__ __forceinline__ float exp_taylor(float x) { return fmaf(x, fmaf(x, fmaf(x, 1.f / 6.f, 0.5f), 1.f), 1.f); }
 
 // One cell: v = (a, b) at the start of the substep, V the trap potential.
 __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupParamsF &P)
@@ -64,12 +55,23 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupP
     for (int it = 0; it < P.itmax; ++it) {
         const float na = xa.x * xa.x + xa.y * xa.y;
         const float nb = xb.x * xb.x + xb.y * xb.y;
-        const float pa_re = -(P.l111 * na * na + P.l12 * nb) * 0.5f;
-        const float pa_im = V + P.g11 * na + P.g12 * nb;
-        const float pb_re = -(P.l22 * nb + P.l12 * na) * 0.5f;
-        const float pb_im = V + P.g22 * nb + P.g12 * na - P.detuning;
-        const float2 ea = cis_small(pa_im * hdt), eb = cis_small(pb_im * hdt);
-        const float ma = exp_small(pa_re * hdt), mb = exp_small(pb_re * hdt);
+        const float ra = -(P.l111 * na * na + P.l12 * nb) * 0.5f * hdt;
+        const float ta = (V + P.g11 * na + P.g12 * nb) * hdt;
+        const float rb = -(P.l22 * nb + P.l12 * na) * 0.5f * hdt;
+        const float tb = (V + P.g22 * nb + P.g12 * na - P.detuning) * hdt;
+        float2 ea, eb;
+        float ma, mb;
+        if (fmaxf(fabsf(ta), fabsf(tb)) <= 0.5f && fmaxf(fabsf(ra), fabsf(rb)) <= 0.015625f) {
+            ea = cis_taylor(ta);
+            eb = cis_taylor(tb);
+            ma = exp_taylor(ra);
+            mb = exp_taylor(rb);
+        } else {
+            sincosf(ta, &ea.y, &ea.x);
+            sincosf(tb, &eb.y, &eb.x);
+            ma = expf(ra);
+            mb = expf(rb);
+        }
         da = make_float2(ma * ea.x, ma * ea.y);
         db = make_float2(mb * eb.x, mb * eb.y);
         xa = cmul(a0, da);
