@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, in
             const float Z = -P.zmax + P.dz * (float)z;
             const float base = Y * Y + Z * Z * P.inv_lambda2;
             const uint32_t tl = (uint32_t)tlocal[traj];
-            const LossAmps A = loss_amps(P);
+            const CellConsts K = cell_consts(P);
             const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
             // cells in pairs: the two Philox draws interleave (loss_noise_cell2)
 #pragma unroll 1
@@ -93,10 +93,10 @@ __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, in
                 const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
                 float4 *s0 = s + c * N + (x ^ (c & 7)), *s1 = s + c * N + ((x + 1) ^ (c & 7));
                 const float4 v0 = *s0, v1 = *s1;
-                float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), P);
-                float4 o1 = nonlinear_cell(v1, 0.5f * (X1 * X1 + base), P);
+                float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
+                float4 o1 = nonlinear_cell(v1, 0.5f * (X1 * X1 + base), K);
                 if (P.noise)
-                    loss_noise_cell2(o0, v0, o1, v1, A, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
+                    loss_noise_cell2(o0, v0, o1, v1, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
                 *s0 = o0;
                 *s1 = o1;
             }
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ stat
         const float Z = -P.zmax + P.dz * (float)z;
         const float base = Y * Y + Z * Z * P.inv_lambda2;
         const uint32_t tl = (uint32_t)tlocal[traj];
-        const LossAmps A = loss_amps(P);
+        const CellConsts K = cell_consts(P);
         const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
         // one cell an iteration: the paired form of k_plane (two interleaved Philox draws) measured
         // 13 % slower here, at the 128-register cap of 8 CTAs per SM
@@ -280,8 +280,8 @@ __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ stat
             const float X = -P.xmax + P.dx * (float)x;
             float4 *slot = tile + tix(r, x);
             const float4 v0 = *slot;
-            float4 o = nonlinear_cell(v0, 0.5f * (X * X + base), P);
-            if (P.noise) o = loss_noise_cell(o, v0, A, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
+            float4 o = nonlinear_cell(v0, 0.5f * (X * X + base), K);
+            if (P.noise) o = loss_noise_cell(o, v0, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
             *slot = o;
         }
 #pragma unroll

@@ -18,13 +18,44 @@
 #include "common.cuh"
 #include "engine.h"
 
-// One Box-Muller pair of loss_normals6 scaled by amp, with the SFU log2/rsqrt/sin/cos:
-// r = amp sqrt(-2 ln u1), u1 = (f1 + 1/2) / 2^21 in (0, 1) so -2 ln u1 > 0 and the square root
-// is taken as y rsqrt(y); (n1, n2) = r (cos, sin)(2 pi f2 / 2^21).
-__device__ __forceinline__ float2 box_muller21_scaled(uint32_t f1, uint32_t f2, float amp)
+// Per-thread constants of a trajectory's cell step, computed once per thread from its GroupParamsF:
+// the nonlinear coefficients scaled by dt/2 and the squared loss-noise amplitudes.
+struct CellConsts {
+    float hdt;                      // dt / 2
+    float hg11, hg12, hg22, hdet;   // g_ij dt/2, detuning dt/2
+    float hl111, hl12, hl22;        // -l dt/4 (the drift -(l111 na^2 + l12 nb)/2 times dt/2)
+    float n1, n2, n3;               // -2 ln 2 (noise_amp c_i)^2
+    int itmax;
+};
+
+__device__ __forceinline__ CellConsts cell_consts(const GroupParamsF &P)
 {
-    const float y = -1.38629436112f * __log2f(fmaf((float)f1, 0x1p-21f, 0x1p-22f));
-    const float r = amp * (y * rsqrtf(y));
+    CellConsts K;
+    K.hdt = 0.5f * P.dt;
+    K.hg11 = P.g11 * K.hdt;
+    K.hg12 = P.g12 * K.hdt;
+    K.hg22 = P.g22 * K.hdt;
+    K.hdet = P.detuning * K.hdt;
+    K.hl111 = -0.5f * K.hdt * P.l111;
+    K.hl12 = -0.5f * K.hdt * P.l12;
+    K.hl22 = -0.5f * K.hdt * P.l22;
+    const float a1 = P.noise_amp * P.c1, a2 = P.noise_amp * P.c2, a3 = P.noise_amp * P.c3;
+    K.n1 = -1.38629436112f * a1 * a1;
+    K.n2 = -1.38629436112f * a2 * a2;
+    K.n3 = -1.38629436112f * a3 * a3;
+    K.itmax = P.itmax;
+    return K;
+}
+
+// One Box-Muller pair of loss_normals6 scaled by an amplitude amp, with the SFU log2/sqrt/sin/cos:
+// r = amp sqrt(-2 ln u1) = sqrt(n log2 u1) for n = -2 ln 2 amp^2, u1 = (f1 + 1/2) / 2^21 in (0, 1);
+// (n1, n2) = r (cos, sin)(2 pi f2 / 2^21). log2 u1 < 0 for every u1 here: its largest value,
+// log2(1 - 2^-22) = -3.4e-7, is twice the SFU log2's absolute error bound on [0.5, 2].
+__device__ __forceinline__ float2 box_muller21_scaled(uint32_t f1, uint32_t f2, float n)
+{
+    const float y = n * __log2f(fmaf((float)f1, 0x1p-21f, 0x1p-22f));
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
     float s, c;
     __sincosf((float)f2 * (6.28318530717958648f * 0x1p-21f), &s, &c);
     return make_float2(r * c, r * s);
@@ -47,18 +78,18 @@ __device__ __forceinline__ float2 cis_taylor(float t)
 __device__ __forceinline__ float exp_taylor(float x) { return fmaf(x, fmaf(x, fmaf(x, 1.f / 6.f, 0.5f), 1.f), 1.f); }
 
 // One cell: v = (a, b) at the start of the substep, V the trap potential.
-__device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupParamsF &P)
+__device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const CellConsts &K)
 {
     const float2 a0 = make_float2(v.x, v.y), b0 = make_float2(v.z, v.w);
-    const float hdt = P.dt * 0.5f;
+    const float hV = V * K.hdt, hVd = hV - K.hdet;
     float2 xa = a0, xb = b0, da = make_float2(0.f, 0.f), db = make_float2(0.f, 0.f);
-    for (int it = 0; it < P.itmax; ++it) {
+    for (int it = 0; it < K.itmax; ++it) {
         const float na = xa.x * xa.x + xa.y * xa.y;
         const float nb = xb.x * xb.x + xb.y * xb.y;
-        const float ra = -(P.l111 * na * na + P.l12 * nb) * 0.5f * hdt;
-        const float ta = (V + P.g11 * na + P.g12 * nb) * hdt;
-        const float rb = -(P.l22 * nb + P.l12 * na) * 0.5f * hdt;
-        const float tb = (V + P.g22 * nb + P.g12 * na - P.detuning) * hdt;
+        const float ra = fmaf(K.hl111 * na, na, K.hl12 * nb);
+        const float rb = fmaf(K.hl22, nb, K.hl12 * na);
+        const float ta = fmaf(K.hg11, na, fmaf(K.hg12, nb, hV));
+        const float tb = fmaf(K.hg22, nb, fmaf(K.hg12, na, hVd));
         float2 ea, eb;
         float ma, mb;
         if (fmaxf(fabsf(ta), fabsf(tb)) <= 0.5f && fmaxf(fabsf(ra), fabsf(rb)) <= 0.015625f) {
@@ -81,41 +112,37 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const GroupP
     return make_float4(ao.x, ao.y, bo.x, bo.y);
 }
 
-// Loss-noise amplitudes of a trajectory: noise_amp x (c1, c2, c3), computed once per thread.
-struct LossAmps { float w1, w2, w3; };
-__device__ __forceinline__ LossAmps loss_amps(const GroupParamsF &P)
-{
-    return LossAmps{P.noise_amp * P.c1, P.noise_amp * P.c2, P.noise_amp * P.c3};
-}
-
-// The increment of loss_noise_cell from a given Philox output.
-__device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const LossAmps &A, u32x4 w)
+// The increment of loss_noise_cell from a given Philox output, accumulated into out as FMA chains:
+//   a += conj(a0)^2 w1 + conj(b0) w2,  b += conj(a0) w2 + conj(b0) w3.
+__device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const CellConsts &K, u32x4 w)
 {
     uint32_t f[6];
     loss_fields(w, f);
-    const float2 w1 = box_muller21_scaled(f[0], f[1], A.w1);
-    const float2 w2 = box_muller21_scaled(f[2], f[3], A.w2);
-    const float2 w3 = box_muller21_scaled(f[4], f[5], A.w3);
-    const float2 ca = make_float2(v0.x, -v0.y), cb = make_float2(v0.z, -v0.w);
-    const float2 da = cadd(cmul(cmul(ca, ca), w1), cmul(cb, w2));
-    const float2 db = cadd(cmul(ca, w2), cmul(cb, w3));
-    return make_float4(out.x + da.x, out.y + da.y, out.z + db.x, out.w + db.y);
+    const float2 w1 = box_muller21_scaled(f[0], f[1], K.n1);
+    const float2 w2 = box_muller21_scaled(f[2], f[3], K.n2);
+    const float2 w3 = box_muller21_scaled(f[4], f[5], K.n3);
+    const float ax = v0.x, ay = v0.y, bx = v0.z, by = v0.w;
+    const float qx = fmaf(ax, ax, -ay * ay), qy = -2.f * ax * ay;       // conj(a0)^2
+    return make_float4(fmaf(qx, w1.x, fmaf(-qy, w1.y, fmaf(bx, w2.x, fmaf(by, w2.y, out.x)))),
+                       fmaf(qx, w1.y, fmaf(qy, w1.x, fmaf(bx, w2.y, fmaf(-by, w2.x, out.y)))),
+                       fmaf(ax, w2.x, fmaf(ay, w2.y, fmaf(bx, w3.x, fmaf(by, w3.y, out.z)))),
+                       fmaf(ax, w2.y, fmaf(-ay, w2.x, fmaf(bx, w3.y, fmaf(-by, w3.x, out.w)))));
 }
 
 // loss_noise_cell for two cells of the same trajectory and step (interleaved Philox draws).
-__device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4 &out1, float4 v1, const LossAmps &A,
+__device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4 &out1, float4 v1, const CellConsts &K,
                                                  uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
                                                  uint32_t cell0, uint32_t cell1)
 {
     const u32x4x2 w = philox4x32_10_x2(cell0, step, traj, RNG_TAG_LOSS, cell1, step, traj, RNG_TAG_LOSS, k0, k1);
-    out0 = loss_noise_apply(out0, v0, A, w.a);
-    out1 = loss_noise_apply(out1, v1, A, w.b);
+    out0 = loss_noise_apply(out0, v0, K, w.a);
+    out1 = loss_noise_apply(out1, v1, K, w.b);
 }
 
 // Adds the loss-noise increment evaluated at v0 to out: the six normals of one Philox4x32-10 draw
 // (loss_fields) as three complex Wiener increments w1, w2, w3 already scaled by their amplitudes.
-__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const LossAmps &A, uint32_t k0,
+__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const CellConsts &K, uint32_t k0,
                                                   uint32_t k1, uint32_t traj, uint32_t step, uint32_t cell)
 {
-    return loss_noise_apply(out, v0, A, philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1));
+    return loss_noise_apply(out, v0, K, philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1));
 }
