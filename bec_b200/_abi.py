@@ -21,6 +21,10 @@ STATUS_NAMES = {
     6: "BEC_ERR_NUMERICAL", 7: "BEC_ERR_NO_DEVICE", 8: "BEC_ERR_UNIMPLEMENTED",
 }
 
+# host element types of bec_init_groups
+BEC_HOST_C128 = 0
+BEC_HOST_C64 = 1
+
 BEC_PATH_FP64_PLAIN = 0
 BEC_PATH_FP32_BATCHED = 1
 

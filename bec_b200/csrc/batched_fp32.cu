@@ -71,6 +71,31 @@ __global__ void k_init(float4 *state, int cells, int ne, GroupParamsF gp, const 
     }
 }
 
+// The same initial state as k_init for a run of trajectories of one grid class that may belong to many
+// ensembles: trajectory t of the run takes its ensemble's parameters gp[tgroup[t]], its ground state
+// gs_ptrs[tgroup[t]] (complex128 or, with T = float2, complex64), and its Philox stream tlocal[t].
+template <typename T>
+__global__ void k_init_batched(float4 *state, int cells, int n_traj, const int *__restrict__ tgroup,
+                               const int *__restrict__ tlocal, const GroupParamsF *__restrict__ gp,
+                               const void *const *__restrict__ gs_ptrs)
+{
+    const size_t n = (size_t)cells * n_traj;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        const int t = (int)(idx / cells);
+        const int i = (int)(idx - (size_t)t * cells);
+        const int grp = tgroup[t];
+        const GroupParamsF &P = gp[grp];
+        float r[4];
+        const uint64_t seed = ((uint64_t)P.seed_hi << 32) | P.seed_lo;
+        normals4<float>(seed, (uint32_t)tlocal[t], 0u, (uint32_t)i, RNG_TAG_INIT, r);
+        const float2 ea = make_float2(0.5f * r[0], 0.5f * r[1]);
+        const float2 eb = make_float2(0.5f * r[2], 0.5f * r[3]);
+        const T g = static_cast<const T *>(gs_ptrs[grp])[i];
+        state[idx] = make_float4((float)g.x + P.init_a * ea.x, (float)g.y + P.init_a * ea.y,
+                                 P.init_b * eb.x, P.init_b * eb.y);
+    }
+}
+
 // ---------------------------------------------------------------- plane pass
 // mode 0: full step (load bit-reversed, FFT_xy, nonlinear, IFFT_xy, store bit-reversed)
 // mode 1: prep (x-space natural in -> IFFT_xy -> stored representation)
@@ -356,6 +381,17 @@ void fp32_init_group(float4 *state, int cells, int ne, const GroupParamsF &gp, c
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 32) blocks = 148 * 32;
     k_init<<<blocks, 256, 0, s>>>(state, cells, ne, gp, gs, noise);
+    g_launches++;
+}
+
+void fp32_init_batched(float4 *state, int cells, int n_traj, const int *tgroup, const int *tlocal,
+                       const GroupParamsF *gp, const void *const *gs_ptrs, bool c64, cudaStream_t s)
+{
+    size_t n = (size_t)cells * n_traj;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (c64) k_init_batched<float2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
+    else k_init_batched<double2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
     g_launches++;
 }
 

@@ -79,6 +79,8 @@ struct bec_ctx {
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
     long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
     GroupParamsF *d_gparams = nullptr;
+    const void **d_gs_ptrs = nullptr;   // batched: device ground-state pointer of every group (bec_init_groups)
+    std::vector<const void *> gs_ptrs_host;   // the table last copied to d_gs_ptrs
     double *d_traj_tot = nullptr;        // [n_traj][4]
     double *d_group_mom = nullptr;       // [n_groups][4]
     int *d_group_first = nullptr, *d_group_count = nullptr;
@@ -1463,6 +1465,86 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
         CKL();
     }
     gr.initialised = true;
+    ctx->last_launches = g_launches - l0;
+    return BEC_OK;
+}
+
+bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const void *const *psi_gs,
+                           int32_t host_type)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (n < 0 || (n > 0 && (!groups || !psi_gs)) || (host_type != BEC_HOST_C128 && host_type != BEC_HOST_C64))
+        return fail(ctx, BEC_ERR_INVALID_ARG, "bad bec_init_groups arguments");
+    const int ng = (int)ctx->groups.size();
+    std::vector<char> listed(ng, 0);
+    for (int i = 0; i < n; ++i) {
+        const int g = groups[i];
+        if (g < 0 || g >= ng || listed[g] || !psi_gs[i])
+            return fail(ctx, BEC_ERR_INVALID_ARG, "bec_init_groups: group index out of range, repeated or NULL");
+        listed[g] = 1;
+    }
+    const bool c64 = host_type == BEC_HOST_C64;
+    bec_status st;
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        const long long l0 = g_launches;
+        for (int i = 0; i < n; ++i) {
+            if (c64) {
+                const int cells = ctx->groups[groups[i]].gd.cells;
+                const float *f = static_cast<const float *>(psi_gs[i]);
+                std::vector<double> d(f, f + 2 * (size_t)cells);
+                if ((st = bec_init_group(ctx, groups[i], d.data(), nullptr))) return st;
+            } else if ((st = bec_init_group(ctx, groups[i], static_cast<const double *>(psi_gs[i]), nullptr))) {
+                return st;
+            }
+        }
+        ctx->last_launches = g_launches - l0;
+        return BEC_OK;
+    }
+    if ((st = batched_resolve(ctx, false))) return st;
+    const long long l0 = g_launches;
+    cudaStream_t s = ctx->stream;
+    if (!ctx->d_gs_ptrs) CKC(dalloc(ctx, &ctx->d_gs_ptrs, (size_t)ng));
+    for (int i = 0; i < n; ++i) {
+        GroupRec &gr = ctx->groups[groups[i]];
+        const size_t cells = (size_t)gr.gd.cells;
+        if (!gr.gs_dev) CKC(dalloc(ctx, &gr.gs_dev, cells));
+        CKC(cudaMemcpyAsync(gr.gs_dev, psi_gs[i], (c64 ? sizeof(float2) : sizeof(double2)) * cells,
+                            cudaMemcpyHostToDevice, s));
+    }
+    // the pointer table follows every gs_dev allocation, bec_init_group's included
+    std::vector<const void *> tab(ng);
+    for (int g = 0; g < ng; ++g) tab[g] = ctx->groups[g].gs_dev;
+    if (tab != ctx->gs_ptrs_host) {
+        // pageable source: the copy is staged before the call returns, so tab may go out of scope
+        CKC(cudaMemcpyAsync(ctx->d_gs_ptrs, tab.data(), sizeof(void *) * ng, cudaMemcpyHostToDevice, s));
+        ctx->gs_ptrs_host = tab;
+    }
+    // one initialisation kernel and one preparation pass per run of consecutive listed trajectories
+    for (auto &c : ctx->classes) {
+        std::vector<std::pair<int, int>> runs;    // (first local trajectory, count)
+        std::vector<int> gl;
+        for (int g : c.groups)
+            if (listed[g]) gl.push_back(g);
+        std::sort(gl.begin(), gl.end(), [&](int a, int b) { return ctx->groups[a].local_first < ctx->groups[b].local_first; });
+        for (int g : gl) {
+            const GroupRec &gr = ctx->groups[g];
+            if (!runs.empty() && runs.back().first + runs.back().second == gr.local_first) runs.back().second += gr.p.ne;
+            else runs.push_back({gr.local_first, gr.p.ne});
+        }
+        for (const auto &r : runs) {
+            float4 *base = c.state + (size_t)r.first * c.geom.cells;
+            fp32_init_batched(base, c.geom.cells, r.second, c.d_tgroup + r.first, c.d_tlocal + r.first, ctx->d_gparams,
+                              ctx->d_gs_ptrs, c64, s);
+            CKL();
+            ClassGeom sub = c.geom;
+            sub.n_traj = r.second;
+            float2 *tx, *ty;
+            if ((st = get_tw32(ctx, sub.nx, &tx)) || (st = get_tw32(ctx, sub.ny, &ty))) return st;
+            fp32_prep(base, sub, tx, ty, s);
+            CKL();
+        }
+    }
+    for (int i = 0; i < n; ++i) ctx->groups[groups[i]].initialised = true;
     ctx->last_launches = g_launches - l0;
     return BEC_OK;
 }

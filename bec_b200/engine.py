@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from ._abi import (BecDerived, BecGsOpts, BecGsReport, BecMoments, BecObs, BecParams, BecSchedule,
-                   BEC_GS_FIXED_STEPS, BEC_LR_CONSTANT, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
+                   BEC_GS_FIXED_STEPS, BEC_HOST_C128, BEC_HOST_C64, BEC_LR_CONSTANT, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbec.so")
@@ -36,6 +36,7 @@ SIGNATURES = {
     "bec_ground_state_batch": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32), _P(BecGsOpts), _P(_dp),
                                          _P(BecGsReport)]),
     "bec_init_group": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp]),
+    "bec_init_groups": (C.c_int, [C.c_void_p, C.c_int32, _P(C.c_int32), _P(C.c_void_p), C.c_int32]),
     "bec_evolve": (C.c_int, [C.c_void_p, C.c_int32]),
     "bec_pulse": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "bec_start_evolution": (C.c_int, [C.c_void_p]),
@@ -205,6 +206,30 @@ class Engine:
         self._check(lib().bec_init_group(self._h, group, _dptr(g.view(np.float64)),
                                          _dptr(nz.view(np.float64)) if nz is not None else None),
                     "bec_init_group")
+
+    def init_groups(self, groups, psi_gs):
+        """bec_init_groups: initialise many groups in one call (vacuum noise from Philox).
+
+        psi_gs[i] is the ground state of groups[i]; complex64 arrays are passed as complex64
+        (half the host-to-device bytes), anything else as complex128. Pinned arrays copy fastest."""
+        groups = [int(g) for g in groups]
+        if len(groups) != len(psi_gs):
+            raise ValueError("one ground state per group")
+        c64 = len(psi_gs) > 0 and all(np.asarray(a).dtype == np.complex64 for a in psi_gs)
+        dt = np.complex64 if c64 else np.complex128
+        arrs = []
+        for g, a in zip(groups, psi_gs):
+            a = np.ascontiguousarray(a, dtype=dt).reshape(-1)
+            if not 0 <= g < self.n_groups:
+                raise ValueError("group index out of range")
+            if a.size != self.derived[g].cells:
+                raise ValueError("ground-state size")
+            arrs.append(a)
+        n = len(groups)
+        gi = (C.c_int32 * max(n, 1))(*groups)
+        ptrs = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrs])
+        self._check(lib().bec_init_groups(self._h, n, gi, ptrs, BEC_HOST_C64 if c64 else BEC_HOST_C128),
+                    "bec_init_groups")
 
     def start_evolution(self):
         self._check(lib().bec_start_evolution(self._h), "bec_start_evolution")

@@ -238,6 +238,22 @@ bec_status bec_warmstart_set_basis(bec_ctx *ctx, int32_t nvx, int32_t nvy, int32
  * ne * 2 * cells interleaved complex values laid out [traj][a|b][cell]. */
 bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise);
 
+/* Host element types of bec_init_groups' ground states */
+enum { BEC_HOST_C128 = 0, BEC_HOST_C64 = 1 };
+
+/* bec_init_group (noise == NULL) for n distinct groups at once: the same initial states bit for
+ * bit. psi_gs[i] is the x-space ground state of groups[i]. It holds cells interleaved complex
+ * values, complex128 (BEC_HOST_C128) or complex64 (BEC_HOST_C64). The batched FP32 path rounds a
+ * ground state to FP32 on the device either way, so complex64 halves the host-to-device copy
+ * without changing any result. The batched path copies every ground state, then launches one
+ * initialisation kernel and one preparation pass per run of consecutive trajectories of a grid
+ * class, not one pair per group. The plain path initialises group by group. BEC_ERR_INVALID_ARG
+ * for an index out of range, a repeated group, a NULL pointer or an unknown host_type.
+ * Extends initEvolution (wigner.cu:202-218) and initializeEnsembles
+ * (wigner_kernel.cu:295-317), which the reference calls once per ensemble. */
+bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const void *const *psi_gs,
+                           int32_t host_type);
+
 /* Advances every trajectory by n real-time split steps (propagate, wigner.cu:178-199). */
 bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps);
 
