@@ -342,6 +342,30 @@ __global__ void k_obs_reduce(const double *part, int tiles, int nz, const double
         for (int k = 0; k < 4; ++k) tot[(size_t)traj * 4 + k] = r.v[k].value();
 }
 
+// FP64 sums of |a|^2, |b|^2 and Re, Im of conj(a) b over the stored state of a class, times `scale`: block
+// `idx` sums range idx % blocks (of `blocks` equal ranges) of trajectory idx / blocks and writes
+// part[idx * 4 + k], the [traj][tile][z = 0][4] layout of k_obs_reduce with `blocks` tiles.
+__global__ void k_state_sums(const float4 *__restrict__ state, int cells, int blocks, double scale,
+                             double *__restrict__ part)
+{
+    const int traj = blockIdx.x / blocks, b = blockIdx.x - traj * blocks;
+    const int chunk = (cells + blocks - 1) / blocks;
+    const int i0 = b * chunk, i1 = min(cells, i0 + chunk);
+    const float4 *p = state + (size_t)traj * cells;
+    KVec<4> acc;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const float4 u = p[i];
+        const double ax = u.x, ay = u.y, bx = u.z, by = u.w;
+        acc.v[0].add(ax * ax + ay * ay);
+        acc.v[1].add(bx * bx + by * by);
+        acc.v[2].add(ax * bx + ay * by);
+        acc.v[3].add(ax * by - ay * bx);
+    }
+    KVec<4> r = block_reduce<4>(acc);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) part[(size_t)blockIdx.x * 4 + k] = r.v[k].value() * scale;
+}
+
 __global__ void k_group_reduce(const double *traj_tot, const int *first, const int *count, double *out)
 {
     const int gidx = blockIdx.x;
@@ -455,6 +479,14 @@ void obs_reduce(const double *obs_partial, int n_traj, int tiles, int nz, const 
 {
     if (n_traj <= 0) return;
     k_obs_reduce<<<n_traj, 256, 0, s>>>(obs_partial, tiles, nz, traj_scale, traj_axial, traj_tot);
+    g_launches++;
+}
+
+void fp32_state_sums(const float4 *state, int cells, int n_traj, int blocks, double scale, double *part,
+                     cudaStream_t s)
+{
+    if (n_traj <= 0) return;
+    k_state_sums<<<n_traj * blocks, 256, 0, s>>>(state, cells, blocks, scale, part);
     g_launches++;
 }
 

@@ -394,6 +394,29 @@ bec_status batched_reduce_obs(bec_ctx *ctx)
     return BEC_OK;
 }
 
+// Moments of the step boundary while the step's second half kick is still pending (no pulse waiting),
+// without ending the step. The pending kick multiplies every k-space amplitude of both components by
+// the same unit-modulus factor, so |a|^2, |b|^2 and conj(a) b summed over the trajectory are those of
+// the stored state (Parseval), which is nx ny times the normalised ifft_xy representation of the
+// observing z pass: the sums are scaled by 1 / (nx ny)^2 and then reduced like an observing pass.
+bec_status batched_moments_stored(bec_ctx *ctx)
+{
+    for (auto &c : ctx->classes) {
+        if (c.geom.n_traj == 0) continue;
+        const int blocks = std::max(1, std::min({64, c.geom.cells / 4096, c.geom.nz}));
+        const double inv = 1.0 / ((double)c.geom.nx * (double)c.geom.ny);
+        fp32_state_sums(c.state, c.geom.cells, c.geom.n_traj, blocks, inv * inv, c.obs_partial, ctx->stream);
+        CKL();
+        obs_reduce(c.obs_partial, c.geom.n_traj, blocks, 1, c.d_traj_scale, nullptr,
+                   ctx->d_traj_tot + (size_t)c.traj_offset * 4, ctx->stream);
+        CKL();
+    }
+    group_reduce(ctx->d_traj_tot, ctx->d_group_first, ctx->d_group_count, (int)ctx->groups.size(),
+                 ctx->d_group_mom, ctx->stream);
+    CKL();
+    return BEC_OK;
+}
+
 // Brings the batched state to a step boundary with no pending kick or pulse.
 bec_status batched_resolve(bec_ctx *ctx, bool observe)
 {
@@ -1781,13 +1804,22 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
         auto event_before = [&](int j) {
             return ((j - 1) > 0 && (j - 1) % every == 0 && sample < n_samples) || j - 1 == sch->pi_pulse_step;
         };
+        // a moments-only sample between steady steps sums the stored state and leaves the step running;
+        // otherwise a pass that ends the step observes the boundary (axial profiles need x-space along z)
+        auto sample_boundary = [&]() -> bec_status {
+            bec_status st2;
+            if (!sch->axial && ctx->pending && !ctx->has_pulse) {
+                if ((st2 = batched_moments_stored(ctx))) return st2;
+            } else {
+                if ((st2 = batched_resolve(ctx, true))) return st2;
+                if ((st2 = batched_reduce_obs(ctx))) return st2;
+            }
+            return take_sample();
+        };
         int i = 1;
         while (i <= n) {
             if (obs_due) {
-                // observe the boundary after step i-1 with a pass that ends that step
-                if ((st = batched_resolve(ctx, true))) return st;
-                if ((st = batched_reduce_obs(ctx))) return st;
-                if ((st = take_sample())) return st;
+                if ((st = sample_boundary())) return st;
                 obs_due = false;
             }
             // a pi pulse scheduled after step i-1 rides on this step's pencil pass (after any sample)
@@ -1807,11 +1839,7 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
             i += len;
             if ((i - 1) % every == 0 && sample < n_samples) obs_due = true;
         }
-        if (obs_due) {
-            if ((st = batched_resolve(ctx, true))) return st;
-            if ((st = batched_reduce_obs(ctx))) return st;
-            if ((st = take_sample())) return st;
-        }
+        if (obs_due && (st = sample_boundary())) return st;
         if (n == sch->pi_pulse_step && (st = apply_pulse(ctx, pi_m))) return st;
     }
     CKC(cudaEventRecord(ctx->ev1, ctx->stream));

@@ -118,6 +118,10 @@ int fp32_zpass_tiles(const ClassGeom &c);   // tiles per trajectory of the z pas
 void obs_reduce(const double *obs_partial, int n_traj, int tiles, int nz, const double *traj_scale,
                 double *traj_axial, double *traj_tot, cudaStream_t s);
 // group sums: for g: out[g][4] = sum_{t in group} traj_tot[t]; trajectories of a group are contiguous
+// FP64 sums (|a|^2, |b|^2, conj(a) b) of every trajectory's stored state in `blocks` ranges each, times scale,
+// into part[traj][block][4] (k_obs_reduce's layout with `blocks` tiles and nz = 1)
+void fp32_state_sums(const float4 *state, int cells, int n_traj, int blocks, double scale, double *part,
+                     cudaStream_t s);
 void group_reduce(const double *traj_tot, const int *group_first, const int *group_count, int n_groups,
                   double *out, cudaStream_t s);
 
