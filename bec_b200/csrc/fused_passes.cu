@@ -121,24 +121,25 @@ __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, in
 // so more warps fit on an SM. Forward transforms are split by decimation in time: x[2j + h] in, a
 // local 16-point DFT, one exchange of 8 values through shared memory, X[k] out in the block layout
 // kblk(s, h) (h = 0: k = 0..7, 16..23; h = 1: k = 8..15, 24..31). Inverse transforms use decimation
-// in frequency through IFFT(v) = conj(FFT(conj v)): block layout in, x[2m + h] out, which is the
-// layout the next forward step expects. The 32 x 32 float4 tile is swizzled like k_plane's.
+// in frequency with the conjugate twiddles: block layout in, x[2m + h] out, which is the layout the
+// next forward step expects. (Written as conj(FFT(conj v)) instead, the sign flips cost a 52-byte
+// register spill and 4 % of the kernel's time.) The 32 x 32 float4 tile is swizzled like k_plane's.
 namespace split32 {
 
 __device__ __forceinline__ int kblk(int s, int h) { return s < 8 ? s + 8 * h : s + 8 + 8 * h; }
 __device__ __forceinline__ int tix(int row, int col) { return row * 32 + (col ^ (row & 7)); }
 
-// v * e^{-2 pi i K / 32}
-template <int K>
+// v * e^{-2 pi i K / 32} (v * e^{+2 pi i K / 32} when INV)
+template <int K, bool INV = false>
 __device__ __forceinline__ float4 w32(float4 v)
 {
     if constexpr (K == 0) {
         return v;
     } else if constexpr (K == 8) {
-        return fftreg::mul_negi(v);
+        return INV ? fftreg::mul_posi(v) : fftreg::mul_negi(v);
     } else {
         constexpr float c = (float)fftreg::cos_2pi(K, 32), sn = (float)fftreg::sin_2pi(K, 32);
-        return fftreg::cmulc(v, c, -sn);
+        return fftreg::cmulc(v, c, INV ? sn : -sn);
     }
 }
 
@@ -167,7 +168,7 @@ template <int H, int I>
 __device__ __forceinline__ void dif_send_one(float4 *v, float4 *xo)
 {
     const float4 a = fftreg::add(v[I], v[8 + I]);
-    const float4 b = w32<H == 0 ? I : 8 + I>(fftreg::sub(v[I], v[8 + I]));
+    const float4 b = w32<H == 0 ? I : 8 + I, true>(fftreg::sub(v[I], v[8 + I]));
     if constexpr (H == 0) {
         v[I] = a;
         xo[I * 32] = b;
@@ -210,8 +211,6 @@ __device__ __forceinline__ void fwd_line(float4 *v, float4 *xb, int h, int lane)
 // inverse (unnormalised): v[s] = x[kblk(s, h)] -> v[m] = y[2m + h]
 __device__ __forceinline__ void inv_line(float4 *v, float4 *xb, int h, int lane)
 {
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
     float4 *xo = xb + h * 256 + lane;
     const float4 *xi = xb + (1 - h) * 256 + lane;
     if (h == 0) dif_send<0>(v, xo, Seq8{});
@@ -219,9 +218,7 @@ __device__ __forceinline__ void inv_line(float4 *v, float4 *xb, int h, int lane)
     __syncthreads();
     if (h == 0) dif_recv<0>(v, xi, Seq8{});
     else dif_recv<1>(v, xi, Seq8{});
-    dft<16, false>(v);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
+    dft<16, true>(v);
 }
 
 } // namespace split32
