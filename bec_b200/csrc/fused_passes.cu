@@ -54,21 +54,13 @@ __global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, in
 #pragma unroll
     for (int y = 0; y < N; ++y) v[y] = g[y * N + c];
 
-    // Four transforms share one code body (the kernel is otherwise bound by
+    // Four transforms share one loop body (the kernel is otherwise bound by
     // instruction fetch): pass 0 forward along y, pass 1 forward along x,
-    // passes 2 and 3 inverse along x and y through IFFT(v) = conj(FFT(conj v)).
+    // passes 2 and 3 inverse along x and y (the inverse DFT body, no sign flips).
 #pragma unroll 1
     for (int pass = 0; pass < 4; ++pass) {
-        const bool inv = pass >= 2;
-        if (inv) {
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
-        }
-        dft<N, false>(v);
-        if (inv) {
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = make_float4(v[i].x, -v[i].y, v[i].z, -v[i].w);
-        }
+        if (pass >= 2) dft<N, true>(v);
+        else dft<N, false>(v);
         if (pass == 0) {
             // column c -> row c
 #pragma unroll
@@ -269,17 +261,19 @@ __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ stat
         const uint32_t tl = (uint32_t)tlocal[traj];
         const CellConsts K = cell_consts(P);
         const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
-        // one cell an iteration: the paired form of k_plane (two interleaved Philox draws) measured
-        // 13 % slower here, at the 128-register cap of 8 CTAs per SM
+        // cells in pairs (x, x + 1; kblk keeps pairs of even s adjacent): the two Philox draws interleave
 #pragma unroll 1
-        for (int s = 0; s < 16; ++s) {
+        for (int s = 0; s < 16; s += 2) {
             const int x = kblk(s, h);
-            const float X = -P.xmax + P.dx * (float)x;
-            float4 *slot = tile + tix(r, x);
-            const float4 v0 = *slot;
-            float4 o = nonlinear_cell(v0, 0.5f * (X * X + base), K);
-            if (P.noise) o = loss_noise_cell(o, v0, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
-            *slot = o;
+            const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
+            float4 *s0 = tile + tix(r, x), *s1 = tile + tix(r, x + 1);
+            const float4 v0 = *s0, v1 = *s1;
+            float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
+            float4 o1 = nonlinear_cell(v1, 0.5f * (X1 * X1 + base), K);
+            if (P.noise)
+                loss_noise_cell2(o0, v0, o1, v1, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
+            *s0 = o0;
+            *s1 = o1;
         }
 #pragma unroll
         for (int s = 0; s < 16; ++s) v[s] = tile[tix(r, kblk(s, h))];
