@@ -207,11 +207,17 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def physical_gpu_index(dev):
+    """nvidia-smi index of CUDA device `dev` (nvidia-smi ignores CUDA_VISIBLE_DEVICES)."""
+    entries = [e.strip() for e in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if e.strip()]
+    if dev < len(entries) and entries[dev].isdigit():
+        return int(entries[dev])
+    return dev
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
-    if ws > 1:
-        os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
     if args.impl == "reference":
         if ws > 1:
             import torch.distributed as dist
@@ -227,7 +233,10 @@ def main():
     from bec_b200.configs import config2
     from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
 
-    torch.cuda.set_device(0 if ws > 1 else 0)
+    # one GPU per rank: LOCAL_RANK among the visible devices (every GPU stays visible, so NCCL sees its
+    # peers), or device 0 when the launcher already gives each rank a single visible GPU
+    dev = local if local < torch.cuda.device_count() else 0
+    torch.cuda.set_device(dev)
     if ws > 1:
         import datetime
         import torch.distributed as dist
@@ -253,7 +262,7 @@ def main():
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
-    with ClockSampler(local) as clk:
+    with ClockSampler(physical_gpu_index(dev)) as clk:
         eng.evolve(args.steps)
         torch.cuda.synchronize()
     ms = eng.last_device_ms
