@@ -45,7 +45,7 @@ struct GroupRec {
     int traj_first = 0;       // global trajectory index of the first trajectory
     int local_first = 0;      // index within the class
     double2 *a = nullptr, *b = nullptr;   // plain path: k-space state [ne][cells]
-    double2 *gs_dev = nullptr;            // batched path: x-space ground state
+    double2 *gs_dev = nullptr;            // batched path: x-space ground state (in the context's gs_stage)
     bool initialised = false;
 };
 
@@ -81,6 +81,7 @@ struct bec_ctx {
     GroupParamsF *d_gparams = nullptr;
     const void **d_gs_ptrs = nullptr;   // batched: device ground-state pointer of every group (bec_init_groups)
     std::vector<const void *> gs_ptrs_host;   // the table last copied to d_gs_ptrs
+    char *gs_stage = nullptr;            // batched: ground states of an init call, in group order (16 B per cell)
     double *d_traj_tot = nullptr;        // [n_traj][4]
     double *d_group_mom = nullptr;       // [n_groups][4]
     int *d_group_first = nullptr, *d_group_count = nullptr;
@@ -1425,6 +1426,20 @@ bec_status bec_ground_state_batch(bec_ctx *ctx, int32_t n, const int32_t *groups
 }
 
 // ------------------------------------------------------------------------ evolution
+namespace {
+// The staging area of the ground states an init call copies to the device: every group's slot in group
+// order, 16 bytes per cell. A ground state is consumed by the call that copies it, so bec_init_group and
+// bec_init_groups share the area; whichever runs first allocates it.
+bec_status gs_stage_ready(bec_ctx *ctx)
+{
+    if (ctx->gs_stage) return BEC_OK;
+    size_t total = 0;
+    for (auto &gr : ctx->groups) total += sizeof(double2) * (size_t)gr.gd.cells;
+    CKC(dalloc(ctx, &ctx->gs_stage, total));
+    return BEC_OK;
+}
+} // namespace
+
 bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise)
 {
     if (!ctx) return BEC_ERR_INVALID_ARG;
@@ -1461,7 +1476,10 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
     } else {
         // bring the other groups to a clean step boundary first
         if ((st = batched_resolve(ctx, false))) return st;
-        if (!gr.gs_dev) CKC(dalloc(ctx, &gr.gs_dev, (size_t)cells));
+        if ((st = gs_stage_ready(ctx))) return st;
+        size_t off = 0;
+        for (int g = 0; g < group; ++g) off += sizeof(double2) * (size_t)ctx->groups[g].gd.cells;
+        gr.gs_dev = reinterpret_cast<double2 *>(ctx->gs_stage + off);
         CKC(cudaMemcpyAsync(gr.gs_dev, psi_gs, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
         float2 *nz = nullptr;
         if (noise) {
@@ -1527,16 +1545,24 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
     const long long l0 = g_launches;
     cudaStream_t s = ctx->stream;
     if (!ctx->d_gs_ptrs) CKC(dalloc(ctx, &ctx->d_gs_ptrs, (size_t)ng));
-    for (int i = 0; i < n; ++i) {
-        GroupRec &gr = ctx->groups[groups[i]];
-        const size_t cells = (size_t)gr.gd.cells;
-        if (!gr.gs_dev) CKC(dalloc(ctx, &gr.gs_dev, cells));
-        CKC(cudaMemcpyAsync(gr.gs_dev, psi_gs[i], (c64 ? sizeof(float2) : sizeof(double2)) * cells,
+    // the staging area holds the listed ground states in group order at the call's element size, so that
+    // consecutive groups whose host buffers are adjacent arrive in one copy
+    const size_t esz = c64 ? sizeof(float2) : sizeof(double2);
+    std::vector<size_t> off(ng + 1, 0);
+    for (int g = 0; g < ng; ++g) off[g + 1] = off[g] + esz * (size_t)ctx->groups[g].gd.cells;
+    if ((st = gs_stage_ready(ctx))) return st;
+    for (int i = 0; i < n;) {
+        int k = i + 1;
+        const char *h0 = static_cast<const char *>(psi_gs[i]);
+        while (k < n && groups[k] == groups[k - 1] + 1 &&
+               static_cast<const char *>(psi_gs[k]) == h0 + (off[groups[k]] - off[groups[i]]))
+            ++k;
+        CKC(cudaMemcpyAsync(ctx->gs_stage + off[groups[i]], h0, off[groups[k - 1] + 1] - off[groups[i]],
                             cudaMemcpyHostToDevice, s));
+        i = k;
     }
-    // the pointer table follows every gs_dev allocation, bec_init_group's included
     std::vector<const void *> tab(ng);
-    for (int g = 0; g < ng; ++g) tab[g] = ctx->groups[g].gs_dev;
+    for (int g = 0; g < ng; ++g) tab[g] = ctx->gs_stage + off[g];
     if (tab != ctx->gs_ptrs_host) {
         // pageable source: the copy is staged before the call returns, so tab may go out of scope
         CKC(cudaMemcpyAsync(ctx->d_gs_ptrs, tab.data(), sizeof(void *) * ng, cudaMemcpyHostToDevice, s));

@@ -299,11 +299,14 @@ def main():
 
     # e2e through the C ABI: host ground states (pinned, complex64: the FP32 path rounds them to FP32 on
     # the device either way) -> one batched init of every ensemble -> pi/2 -> K steps -> moments to host
-    host_gs64 = []
+    # one pinned buffer, the groups' ground states back to back in group order (bec_init_groups then
+    # copies them in one transfer)
+    pin = torch.empty(2 * sum(a.size for a in host_gs), dtype=torch.float32, pin_memory=True).numpy().view(np.complex64)
+    host_gs64, o = [], 0
     for a in host_gs:
-        pin = torch.empty(2 * a.size, dtype=torch.float32, pin_memory=True).numpy().view(np.complex64)
-        pin[:] = a
-        host_gs64.append(pin)
+        pin[o:o + a.size] = a
+        host_gs64.append(pin[o:o + a.size])
+        o += a.size
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()

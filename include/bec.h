@@ -245,7 +245,8 @@ enum { BEC_HOST_C128 = 0, BEC_HOST_C64 = 1 };
  * bit. psi_gs[i] is the x-space ground state of groups[i]. It holds cells interleaved complex
  * values, complex128 (BEC_HOST_C128) or complex64 (BEC_HOST_C64). The batched FP32 path rounds a
  * ground state to FP32 on the device either way, so complex64 halves the host-to-device copy
- * without changing any result. The batched path copies every ground state, then launches one
+ * without changing any result. The batched path copies the ground states (consecutive groups whose host
+ * arrays lie back to back in memory in one transfer), then launches one
  * initialisation kernel and one preparation pass per run of consecutive trajectories of a grid
  * class, not one pair per group. The plain path initialises group by group. BEC_ERR_INVALID_ARG
  * for an index out of range, a repeated group, a NULL pointer or an unknown host_type.

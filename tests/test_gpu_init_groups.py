@@ -66,6 +66,18 @@ def test_batched_init_bit_identical():
     # reversed order of the list, complex64 ground states rounded from the complex128 ones
     assert_same(ref, run(lambda eng, gs: eng.init_groups(list(range(len(gs)))[::-1],
                                                          [a.astype(np.complex64) for a in gs[::-1]])))
+    # ground states back to back in one host buffer: consecutive groups arrive in one copy
+    assert_same(ref, run(lambda eng, gs: eng.init_groups(range(len(gs)), contiguous_views(gs, np.complex64))))
+    assert_same(ref, run(lambda eng, gs: eng.init_groups(range(len(gs)), contiguous_views(gs, np.complex128))))
+
+
+def contiguous_views(arrays, dtype):
+    buf = np.concatenate([a.astype(dtype) for a in arrays])
+    out, o = [], 0
+    for a in arrays:
+        out.append(buf[o:o + a.size])
+        o += a.size
+    return out
 
 
 def test_batched_init_subset():
