@@ -27,7 +27,6 @@ struct GsArgs {
     int measure;              // 1: accumulate sum |psi_k|^2 (and the kinetic sum) per trajectory
 };
 
-__device__ __forceinline__ float2 conj2(float2 v) { return make_float2(v.x, -v.y); }
 
 // ---------------------------------------------------------------- pencil pass
 template <int NZ>
@@ -44,6 +43,8 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
     float2 *tw = buf + 16 * NZ;                  // W_NZ^e
     float *kz2 = reinterpret_cast<float *>(tw + NZ);   // kz^2/2 per kz
     float *kxy2 = kz2 + NZ;                      // (kx^2 + ky^2)/2 per pencil
+    float *ez1 = kxy2 + 16, *ez2 = ez1 + NZ;     // exp(-dt frac1,2 kz^2/2) per kz
+    float *exy1 = ez2 + NZ, *exy2 = exy1 + 16;   // exp(-dt frac1,2 (kx^2 + ky^2)/2) x scale, out_scale
     __shared__ double red[2][NZ / 32];
 
     const int t = threadIdx.x;
@@ -59,6 +60,8 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
         tw[i] = tw_g[i];
         const float kz = getk<float>(i, P.dkz, NZ);
         kz2[i] = 0.5f * kz * kz;
+        ez1[i] = expf(-dts * a.frac1 * kz2[i]);
+        ez2[i] = expf(-dts * a.frac2 * kz2[i]);
     }
     if (t < 16) {
         const int pen = pen0 + t;
@@ -66,6 +69,8 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
         const float kx = getk<float>(x, P.dkx, nx);
         const float ky = (ny > 1) ? getk<float>(y, P.dky, ny) : 0.0f;
         kxy2[t] = 0.5f * (kx * kx + ky * ky);
+        exy1[t] = expf(-dts * a.frac1 * kxy2[t]) * a.scale;
+        exy2[t] = expf(-dts * a.frac2 * kxy2[t]) * a.out_scale;
     }
 
     const int p = t & 15, j = t >> 4;
@@ -93,9 +98,10 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
 #pragma unroll
     for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);
 
-    // propagateKSpaceImaginaryTime (wigner_kernel.cu:128-134): exp(-dt_steady frac k^2/2), real
+    // propagateKSpaceImaginaryTime (wigner_kernel.cu:128-134): exp(-dt_steady frac k^2/2), real, as the
+    // product of its (kx, ky) and kz factors
     double n_acc = 0.0, e_acc = 0.0;
-    const float kxy = kxy2[p2];
+    const float kxy = kxy2[p2], fxy1 = exy1[p2], fxy2 = exy2[p2];
 #pragma unroll
     for (int r = 0; r < R / G; ++r)
 #pragma unroll
@@ -103,14 +109,14 @@ __global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, in
             const int k = q + G * r + R * k2;
             const float k2h = kxy + kz2[k];
             float2 v = y[r * G + k2];
-            const float e1 = expf(-dts * a.frac1 * k2h) * a.scale;
+            const float e1 = fxy1 * ez1[k];
             v = make_float2(v.x * e1, v.y * e1);
             if (a.measure) {
                 const double nk = (double)v.x * v.x + (double)v.y * v.y;
                 n_acc += nk;
                 e_acc += nk * k2h;
             }
-            const float e2 = expf(-dts * a.frac2 * k2h) * a.out_scale;
+            const float e2 = fxy2 * ez2[k];
             y[r * G + k2] = make_float2(v.x * e2, v.y * e2);
         }
     if (a.measure) {
@@ -184,16 +190,8 @@ __global__ void __launch_bounds__(128) k_gs_plane(float2 *__restrict__ state, in
     const int p_end = (MODE == 2) ? 2 : 4;
 #pragma unroll 1
     for (int pass = p_begin; pass < p_end; ++pass) {
-        const bool inv = pass >= 2;
-        if (inv) {
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = conj2(v[i]);
-        }
-        dft<N, false>(v);
-        if (inv) {
-#pragma unroll
-            for (int i = 0; i < N; ++i) v[i] = conj2(v[i]);
-        }
+        if (pass >= 2) dft<N, true>(v);
+        else dft<N, false>(v);
         if (pass == 0) {
 #pragma unroll
             for (int y = 0; y < N; ++y) s[y * N + (c ^ (y & SW))] = v[y];
@@ -316,7 +314,7 @@ void launch_gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp,
                       const int *active, cudaStream_t s)
 {
     const int tiles = c.nx * c.ny / 16;
-    const size_t smem = sizeof(float2) * (16 * NZ + NZ) + sizeof(float) * (NZ + 16);
+    const size_t smem = sizeof(float2) * (16 * NZ + NZ) + sizeof(float) * (3 * NZ + 3 * 16);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gs_pencil<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
