@@ -33,7 +33,7 @@ using fftreg::dft;
 
 // ---------------------------------------------------------------- plane pass
 template <int N>
-__global__ void __launch_bounds__(128, 3) k_plane(float4 *__restrict__ state, int nz, int cells,
+__global__ void __launch_bounds__(128, 4) k_plane(float4 *__restrict__ state, int nz, int cells,
                                                const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
                                                const int *__restrict__ tlocal, const uint32_t *__restrict__ stepp)
 {
