@@ -26,6 +26,7 @@
 #include "engine.h"
 #include "fft_reg.cuh"
 #include "physics.cuh"
+#include "split32.cuh"
 
 namespace {
 
@@ -108,112 +109,9 @@ __global__ void __launch_bounds__(128, 4) k_plane(float4 *__restrict__ state, in
 }
 
 // ---------------------------------------------------------------- plane pass, 32 x 32, two warps a plane
-// The same plane step for N = 32 with every 32-point line shared by lane L of warp 0 and lane L of
-// warp 1 of the plane's CTA (h = warp): each holds 16 elements, half the registers of k_plane<32>,
-// so more warps fit on an SM. Forward transforms are split by decimation in time: x[2j + h] in, a
-// local 16-point DFT, one exchange of 8 values through shared memory, X[k] out in the block layout
-// kblk(s, h) (h = 0: k = 0..7, 16..23; h = 1: k = 8..15, 24..31). Inverse transforms use decimation
-// in frequency with the conjugate twiddles: block layout in, x[2m + h] out, which is the layout the
-// next forward step expects. (Written as conj(FFT(conj v)) instead, the sign flips cost a 52-byte
-// register spill and 4 % of the kernel's time.) The 32 x 32 float4 tile is swizzled like k_plane's.
-namespace split32 {
-
-__device__ __forceinline__ int kblk(int s, int h) { return s < 8 ? s + 8 * h : s + 8 + 8 * h; }
-__device__ __forceinline__ int tix(int row, int col) { return row * 32 + (col ^ (row & 7)); }
-
-// v * e^{-2 pi i K / 32} (v * e^{+2 pi i K / 32} when INV)
-template <int K, bool INV = false>
-__device__ __forceinline__ float4 w32(float4 v)
-{
-    if constexpr (K == 0) {
-        return v;
-    } else if constexpr (K == 8) {
-        return INV ? fftreg::mul_posi(v) : fftreg::mul_negi(v);
-    } else {
-        constexpr float c = (float)fftreg::cos_2pi(K, 32), sn = (float)fftreg::sin_2pi(K, 32);
-        return fftreg::cmulc(v, c, INV ? sn : -sn);
-    }
-}
-
-// decimation in time, after the local DFT16: H = 0 keeps Y0[I] and receives Y1[I] -> X[I], X[16 + I];
-// H = 1 keeps Y1[8 + I] and receives Y0[8 + I] -> X[8 + I], X[24 + I]
-template <int H, int I>
-__device__ __forceinline__ void dit_send_one(const float4 *v, float4 *xo) { xo[I * 32] = H == 0 ? v[8 + I] : v[I]; }
-template <int H, int I>
-__device__ __forceinline__ void dit_recv_one(float4 *v, const float4 *xi)
-{
-    const float4 r = xi[I * 32];
-    const float4 e = H == 0 ? v[I] : r;
-    const float4 o = H == 0 ? r : v[8 + I];
-    constexpr int K = H == 0 ? I : 8 + I;
-    if constexpr (K == 0 || K == 8) {
-        const float4 t = w32<K>(o);
-        v[I] = fftreg::add(e, t);
-        v[8 + I] = fftreg::sub(e, t);
-    } else {
-        fftreg::bfly_w<K, 32, false>(v[I], v[8 + I], e, o);
-    }
-}
-// decimation in frequency, before the local DFT16: n = I (H = 0) or 8 + I (H = 1),
-// a[n] = x[n] + x[n + 16], b[n] = (x[n] - x[n + 16]) W^n; H = 0 gathers a[0..15], H = 1 b[0..15]
-template <int H, int I>
-__device__ __forceinline__ void dif_send_one(float4 *v, float4 *xo)
-{
-    const float4 a = fftreg::add(v[I], v[8 + I]);
-    const float4 b = w32<H == 0 ? I : 8 + I, true>(fftreg::sub(v[I], v[8 + I]));
-    if constexpr (H == 0) {
-        v[I] = a;
-        xo[I * 32] = b;
-    } else {
-        v[8 + I] = b;
-        xo[I * 32] = a;
-    }
-}
-template <int H, int I>
-__device__ __forceinline__ void dif_recv_one(float4 *v, const float4 *xi)
-{
-    if constexpr (H == 0) v[8 + I] = xi[I * 32];
-    else v[I] = xi[I * 32];
-}
-
-template <int H, int... I>
-__device__ __forceinline__ void dit_send(const float4 *v, float4 *xo, std::integer_sequence<int, I...>) { (dit_send_one<H, I>(v, xo), ...); }
-template <int H, int... I>
-__device__ __forceinline__ void dit_recv(float4 *v, const float4 *xi, std::integer_sequence<int, I...>) { (dit_recv_one<H, I>(v, xi), ...); }
-template <int H, int... I>
-__device__ __forceinline__ void dif_send(float4 *v, float4 *xo, std::integer_sequence<int, I...>) { (dif_send_one<H, I>(v, xo), ...); }
-template <int H, int... I>
-__device__ __forceinline__ void dif_recv(float4 *v, const float4 *xi, std::integer_sequence<int, I...>) { (dif_recv_one<H, I>(v, xi), ...); }
-
-using Seq8 = std::make_integer_sequence<int, 8>;
-
-// forward: v[j] = x[2j + h] -> v[s] = X[kblk(s, h)]; xb: the plane's exchange slots [2][8][32]
-__device__ __forceinline__ void fwd_line(float4 *v, float4 *xb, int h, int lane)
-{
-    dft<16, false>(v);
-    float4 *xo = xb + h * 256 + lane;
-    const float4 *xi = xb + (1 - h) * 256 + lane;
-    if (h == 0) dit_send<0>(v, xo, Seq8{});
-    else dit_send<1>(v, xo, Seq8{});
-    __syncthreads();
-    if (h == 0) dit_recv<0>(v, xi, Seq8{});
-    else dit_recv<1>(v, xi, Seq8{});
-}
-
-// inverse (unnormalised): v[s] = x[kblk(s, h)] -> v[m] = y[2m + h]
-__device__ __forceinline__ void inv_line(float4 *v, float4 *xb, int h, int lane)
-{
-    float4 *xo = xb + h * 256 + lane;
-    const float4 *xi = xb + (1 - h) * 256 + lane;
-    if (h == 0) dif_send<0>(v, xo, Seq8{});
-    else dif_send<1>(v, xo, Seq8{});
-    __syncthreads();
-    if (h == 0) dif_recv<0>(v, xi, Seq8{});
-    else dif_recv<1>(v, xi, Seq8{});
-    dft<16, true>(v);
-}
-
-} // namespace split32
+// k_plane's step for N = 32 with the line transforms of split32.cuh: every 32-point line is shared by
+// lane L of warp 0 and lane L of warp 1 of the plane's CTA, 16 elements each, half the registers of a
+// one-lane line, so more warps fit on an SM. The 32 x 32 float4 tile is swizzled like k_plane's.
 
 template <int MINB>
 __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ state, int nz, int cells,
