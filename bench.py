@@ -30,8 +30,8 @@ sys.path.insert(0, ROOT)
 # profiles/pencil_32x32x256.md); traffic scales with the trajectories a launch
 # processes. Algorithmic: 32 B x 262144 cells = 8.39 MB per trajectory.
 NCU_TRAFFIC_PER_TRAJ = {
-    "plane_32x32x256": (268.488704e6 + 208.971520e6) / 64,
-    "pencil_32x32x256": (268.494592e6 + 214.559488e6) / 64,
+    "plane_32x32x256": (268.500224e6 + 210.539776e6) / 64,
+    "pencil_32x32x256": (268.492800e6 + 209.569280e6) / 64,
 }
 
 N_TRAJ = 1024
