@@ -34,6 +34,14 @@ NCU_TRAFFIC_PER_TRAJ = {
     "pencil_32x32x256": (268.492800e6 + 209.569280e6) / 64,
 }
 
+# ncu: thread-instructions per cell of one launch (smsp__inst_executed.sum x 32 / cells), from the same
+# captures. With the launch time they give the kernel's instruction issue rate, whose ceiling is one
+# warp-instruction per scheduler per clock: SMs x 4 x 32 thread-instructions per clock.
+NCU_INSTR_PER_CELL = {
+    "plane_32x32x256": 193569962 * 32 / (64 * 262144),
+    "pencil_32x32x256": 68464640 * 32 / (64 * 262144),
+}
+
 N_TRAJ = 1024
 WORKLOAD = "uneven-ensembles-1024"
 
@@ -361,6 +369,19 @@ def main():
         cpu = {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": s}
 
     clocks = clk.summary()
+    issue_roof = None
+    if dom["kernel"] in NCU_INSTR_PER_CELL:
+        nx, ny, nz = (int(v) for v in dom["kernel"].split("_")[1].split("x"))
+        instr = NCU_INSTR_PER_CELL[dom["kernel"]] * nx * ny * nz * dom["traj"]
+        mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        if mhz:
+            ach = instr / (dom["ms"] * 1e-3)
+            pk = sms * 4 * 32 * mhz * 1e6
+            issue_roof = {"kernel": dom["kernel"], "thread_instructions_per_cell": NCU_INSTR_PER_CELL[dom["kernel"]],
+                          "achieved": ach, "peak": pk, "unit": "thread-instr/s", "frac": ach / pk,
+                          "note": "instruction issue, the bound of this kernel: one warp-instruction per scheduler "
+                                  "per clock at the sampled SM clock; instructions per cell from ncu"}
     if rank == 0:
         line = {
             "metric": "wigner_traj_steps_per_s", "value": value, "unit": "traj-steps/s",
@@ -373,7 +394,8 @@ def main():
                        "trap_jitter": "+-10%", "dt_s": 4e-5, "noise": "Philox vacuum + loss noise",
                        "l2": f"state {16 * total_cells / 1e9:.2f} GB per GPU, larger than L2",
                        "parallelism": f"dp{ws} (trajectory sharding)", "path": "fp32-batched"},
-            "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "issue_roofline": issue_roof, "step_roofline": step_roof, "cpu_baseline": cpu,
+            "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, **extras,
         }
         print(json.dumps(line), flush=True)
