@@ -55,13 +55,13 @@ def copy_params(p, **changes):
     return q
 
 
-def config0():
+def slice_2d_32x128():
     """2D x-z slice, 32x128, one noise-free trajectory, N = 30000:
     2000 imaginary-time steps, pi/2, 100 ms (2500 steps)."""
     return rb87_params(N=30000, grid=(32, 1, 128), ne=1, noise=False)
 
 
-def config1(ne=4, seed=0):
+def ensemble_16x16x128(ne=4, seed=0):
     """3D truncated Wigner, 16x16x128, 4 trajectories, N = 30000, 200 ms."""
     return rb87_params(N=30000, grid=(16, 16, 128), ne=ne, noise=True, seed=seed)
 
@@ -69,7 +69,7 @@ def config1(ne=4, seed=0):
 UNEVEN_GRIDS = ((8, 8, 64), (16, 16, 128), (32, 32, 256))
 
 
-def config2(n_traj=1024, seed=2, grids=UNEVEN_GRIDS):
+def uneven_batch(n_traj=1024, seed=2, grids=UNEVEN_GRIDS):
     """Uneven batch: n_traj single-trajectory ensembles, grid drawn uniformly
     from `grids`, N ~ U[5000, 70000], fx and fz each scaled by U[0.9, 1.1]
     (fy follows fx), noise and losses on. Seeded; returns a list of params."""
@@ -85,7 +85,7 @@ def config2(n_traj=1024, seed=2, grids=UNEVEN_GRIDS):
     return out
 
 
-def config4(ne=1024, seed=4):
+def spin_echo_32x32x256(ne=1024, seed=4):
     """Ramsey / spin echo: N = 70000, 32x32x256, 1024 trajectories, 1.0 s with a
     pi pulse at 0.5 s, final pi/2 sampled at 50 phase points."""
     return rb87_params(N=70000, grid=(32, 32, 256), ne=ne, noise=True, seed=seed)

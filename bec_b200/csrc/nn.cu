@@ -3,7 +3,7 @@
 // No counterpart in the reference. The network maps an ensemble's parameters
 // to the coefficients of a correction to the Thomas-Fermi profile; its output
 // only seeds the imaginary-time ground-state loop (bec_ground_state_batch),
-// which remains the judge of convergence.
+// which alone decides convergence.
 //
 // Layers are Y = act(X W^T + b) (W is [out x in], row-major, as a linear layer),
 // tanh on hidden layers, identity on the last. GEMMs run on the tensor cores with

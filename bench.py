@@ -188,10 +188,10 @@ def cpu_baseline(groups, seconds):
 
 
 def run_reference(args, ws, rank):
-    from bec_b200.configs import config2
+    from bec_b200.configs import uneven_batch
     if rank != 0:
         return
-    groups = config2(n_traj=args.n_traj, seed=2, grids=grid_mix(args))
+    groups = uneven_batch(n_traj=args.n_traj, seed=2, grids=grid_mix(args))
     s = OracleSample(groups)
     for _ in range(args.warmup):
         s.step()
@@ -238,7 +238,7 @@ def main():
 
     import numpy as np
     import torch
-    from bec_b200.configs import config2
+    from bec_b200.configs import uneven_batch
     from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
 
     # one GPU per rank: LOCAL_RANK among the visible devices (every GPU stays visible, so NCCL sees its
@@ -250,7 +250,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    groups = config2(n_traj=args.n_traj, seed=2 + 7919 * rank, grids=grid_mix(args))
+    groups = uneven_batch(n_traj=args.n_traj, seed=2 + 7919 * rank, grids=grid_mix(args))
     eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
     # pinned host ground states (Thomas-Fermi), reused by the e2e leg
     host_gs = []

@@ -354,7 +354,7 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
  * identity on the last), trained and evaluated on the GPU with BF16
  * tensor-core GEMMs accumulating in FP32. No counterpart in the reference: it
  * predicts the coefficients of a correction to the Thomas-Fermi profile that
- * seeds bec_ground_state_batch (warm_start), which stays the judge.
+ * seeds bec_ground_state_batch (warm_start), which alone decides convergence.
  * widths has n_layers + 1 entries (inputs, hidden..., outputs). Host parameter
  * layout: for each layer W [out x in] row-major, then b [out].
  */

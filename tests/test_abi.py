@@ -12,7 +12,7 @@ import pytest
 
 from bec_b200 import _abi
 from bec_b200 import engine as E
-from bec_b200.configs import config0, config1, config2, config4, rb87_params
+from bec_b200.configs import slice_2d_32x128, ensemble_16x16x128, uneven_batch, spin_echo_32x32x256, rb87_params
 from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -63,7 +63,7 @@ int main(void) {
     assert sizes == expect
 
 
-@pytest.mark.parametrize("params", [config0(), config1(), config4(ne=2)] + config2(n_traj=6)
+@pytest.mark.parametrize("params", [slice_2d_32x128(), ensemble_16x16x128(), spin_echo_32x32x256(ne=2)] + uneven_batch(n_traj=6)
                          + [rb87_params(t_equilib=1e-3), rb87_params(grid=(32, 1, 64), fy=50.0)])
 def test_product_derivation_equals_oracle(params):
     d1 = E.derive(params)

@@ -16,7 +16,7 @@ import pytest
 
 from bec_b200 import observables as OBS
 from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_REFERENCE_E
-from bec_b200.configs import config0, config1, copy_params, rb87_params
+from bec_b200.configs import slice_2d_32x128, ensemble_16x16x128, copy_params, rb87_params
 from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
 from oracle import oracle as O
 from parity_util import engine_sequence, moments_rel_err, oracle_sequence, record, rel_state_err
@@ -34,20 +34,20 @@ PATHS = [BEC_PATH_FP64_PLAIN, BEC_PATH_FP32_BATCHED]
 
 
 @pytest.fixture(scope="module")
-def cfg0_gs():
-    p = config0()
+def slice_gs():
+    p = slice_2d_32x128()
     psi, rep = O.ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=2000)
     return p, psi
 
 
 # ------------------------------------------------------------------ ground state
-def test_fp64_ground_state_config0_2000_steps(cfg0_gs):
-    """2D 32x128, 2000 imaginary-time steps from Thomas-Fermi."""
-    p, psi_o = cfg0_gs
+def test_fp64_ground_state_2d_slice_2000_steps(slice_gs):
+    """The 2D 32x128 slice: 2000 imaginary-time steps from Thomas-Fermi."""
+    p, psi_o = slice_gs
     eng = Engine([p], path=BEC_PATH_FP64_PLAIN)
     psi, rep = eng.ground_state(0, mode=BEC_GS_FIXED_STEPS, max_steps=2000)
     err = rel_state_err(psi, psi_o)
-    record("gs_config0_fp64", state_err=err)
+    record("gs_slice2d_fp64", state_err=err)
     assert rep.steps == 2000
     assert err < FP64_TOL
     mu_o, e_o, r_o, n_o = O.gs_measures(p, psi_o)
@@ -84,11 +84,11 @@ def test_ground_state_warm_start():
     assert warm.steps < cold.steps
 
 
-# ------------------------------------------------------------------ configs[0] evolution
+# ------------------------------------------------------------------ 2D 32x128 evolution
 @pytest.mark.parametrize("path", PATHS)
-def test_config0_evolution(cfg0_gs, path):
-    """pi/2 then 100 ms (2500 steps), no noise, samples every 250 steps."""
-    p, gs = cfg0_gs
+def test_2d_slice_evolution(slice_gs, path):
+    """The 2D 32x128 slice: pi/2 then 100 ms (2500 steps), no noise, samples every 250 steps."""
+    p, gs = slice_gs
     mo, eo = oracle_sequence(p, gs, 2500, 250)
     me, ee = engine_sequence(p, gs, 2500, 250, path)
     assert me.shape == mo.shape
@@ -100,7 +100,7 @@ def test_config0_evolution(cfg0_gs, path):
     vis_o = [OBS.visibility(m, d, 1) for m in mo]
     vis_err = float(np.max(np.abs(np.array(vis_e) - np.array(vis_o))))
     st_err = rel_state_err(ee.get_state(0, 0), eo.get_state(0))
-    record(f"config0_path{path}", moments_err=worst_m, vis_err=vis_err, state_err=st_err)
+    record(f"slice2d_path{path}", moments_err=worst_m, vis_err=vis_err, state_err=st_err)
     assert worst_m < tol_m
     assert st_err < (FP64_TOL if path == BEC_PATH_FP64_PLAIN else FP32_STATE_LONG)
     assert vis_err < (1e-10 if path == BEC_PATH_FP64_PLAIN else FP32_VIS)
@@ -254,16 +254,16 @@ def test_state_roundtrip(path):
     assert rel_state_err(back, ab) < (1e-14 if path == BEC_PATH_FP64_PLAIN else 1e-6)
 
 
-def test_paths_agree_on_config1_ensemble_visibility():
-    """configs[1]-shaped run (16x16x128, 4 trajectories, noise), 250 steps: ensemble
+def test_paths_agree_on_16x16x128_ensemble_visibility():
+    """A 16x16x128 ensemble of 4 trajectories with noise, 250 steps: ensemble
     visibility of the batched FP32 path within 1e-3 of the FP64 oracle."""
-    p = config1()
+    p = ensemble_16x16x128()
     gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=400)
     mo, eo = oracle_sequence(p, gs, 250, 50)
     me, ee = engine_sequence(p, gs, 250, 50, BEC_PATH_FP32_BATCHED)
     d = eo.d
     err = max(abs(OBS.visibility(a, d, p.ne) - OBS.visibility(b, d, p.ne)) for a, b in zip(me, mo))
     perr = max(abs(OBS.phase(a) - OBS.phase(b)) for a, b in zip(me, mo))
-    record("config1_vis", vis_err=err, phase_err=perr)
+    record("ensemble16_vis", vis_err=err, phase_err=perr)
     assert err < 1e-3
     assert perr < 1e-3

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from bec_b200 import distributed as D
-from bec_b200.configs import config2
+from bec_b200.configs import uneven_batch
 
 
 def _free_port():
@@ -19,7 +19,7 @@ def _free_port():
 
 
 def test_shard_covers_every_group_once_and_balances():
-    groups = config2(n_traj=97, seed=3)
+    groups = uneven_batch(n_traj=97, seed=3)
     for world in (1, 2, 3, 8):
         owned = [D.shard(groups, r, world) for r in range(world)]
         flat = sorted(i for o in owned for i in o)
@@ -34,7 +34,7 @@ def _worker(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        groups = config2(n_traj=10, seed=5)
+        groups = uneven_batch(n_traj=10, seed=5)
         mine = D.shard(groups, rank, world)
         rng = np.random.default_rng(0)
         allm = rng.standard_normal((3, len(groups), 5))

@@ -10,7 +10,7 @@ import pytest
 
 from bec_b200 import observables as OBS
 from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU, BEC_GS_MU_RESIDUAL, BEC_GS_REFERENCE_E
-from bec_b200.configs import config0, copy_params, rb87_params
+from bec_b200.configs import slice_2d_32x128, copy_params, rb87_params
 from oracle import oracle as O
 
 
@@ -139,7 +139,7 @@ def test_ground_state_converges_and_mu_matches_tf():
 
 
 def test_ground_state_reference_energy_mode_stops():
-    p = config0()
+    p = slice_2d_32x128()
     psi, rep = O.ground_state(p, mode=BEC_GS_REFERENCE_E, max_steps=20000)
     assert rep.converged == 1 and rep.steps < 20000
 
@@ -167,7 +167,7 @@ def test_mu_residual_rule_stops_at_second_check_from_the_fixed_point():
 
 
 def test_imaginary_time_lowers_energy():
-    p = config0()
+    p = slice_2d_32x128()
     _, r1 = O.ground_state(p, max_steps=10)
     _, r2 = O.ground_state(p, max_steps=400)
     assert r2.energy < r1.energy
