@@ -1,0 +1,57 @@
+"""The benchmark's output contract: one JSON line with the keys a driver reads.
+
+The reference arm (the FP64 CPU restatement of the reference's split step) runs here on the CPU on
+a small sample. The GPU arm runs a small workload on a B200. Both must print exactly one JSON line
+with the metric, its unit and the objects the bench line promises.
+"""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def bench_line(args, env=None):
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True, text=True,
+                       cwd=ROOT, env=env, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    return json.loads(lines[0])
+
+
+def test_reference_arm_line():
+    d = bench_line(["--impl", "reference", "--steps", "1", "--warmup", "0", "--n-traj", "8", "--cpu-seconds", "1"])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "wigner_traj_steps_per_s" and d["unit"] == "traj-steps/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_rank_to_physical_gpu(monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.delenv("CUDA_VISIBLE_DEVICES", raising=False)
+    assert bench.physical_gpu_index(3) == 3
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "4,5,6,7")
+    assert bench.physical_gpu_index(0) == 4 and bench.physical_gpu_index(3) == 7
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "GPU-abc")       # UUIDs: fall back to the CUDA index
+    assert bench.physical_gpu_index(0) == 0
+
+
+@pytest.mark.gpu
+def test_gpu_arm_line():
+    d = bench_line(["--steps", "5", "--warmup", "3", "--n-traj", "48", "--no-extras"])
+    assert d["metric"] == "wigner_traj_steps_per_s" and d["value"] > 0 and d["steps"] == 5 and d["warmup"] == 3
+    roof = d["roofline"]
+    assert roof["bound"] == "hbm" and roof["peak"] > 0 and 0 < roof["frac"] == pytest.approx(roof["achieved"] / roof["peak"])
+    e2e = d["e2e"]
+    assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] > 0 and e2e["d2h_bytes_per_step"] > 0
+    assert d["gpu_launches"] > 0
+    if d["clocks"] is not None:                 # None only where nvidia-smi gave no samples
+        assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
