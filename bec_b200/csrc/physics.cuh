@@ -112,7 +112,7 @@ __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const CellCo
     return make_float4(ao.x, ao.y, bo.x, bo.y);
 }
 
-// The increment of loss_noise_cell from a given Philox output, accumulated into out as FMA chains:
+// The loss-noise increment of one cell from its Philox output, accumulated into out as FMA chains:
 //   a += conj(a0)^2 w1 + conj(b0) w2,  b += conj(a0) w2 + conj(b0) w3.
 __device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const CellConsts &K, u32x4 w)
 {
@@ -129,7 +129,9 @@ __device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const 
                        fmaf(ax, w2.y, fmaf(-ay, w2.x, fmaf(bx, w3.y, fmaf(-by, w3.x, out.w)))));
 }
 
-// loss_noise_cell for two cells of the same trajectory and step (interleaved Philox draws).
+// Adds the loss-noise increments of two cells of the same trajectory and step, evaluated at v0 and v1, to
+// out0 and out1: per cell the six normals of one Philox4x32-10 draw (loss_fields) as three complex Wiener
+// increments already scaled by their amplitudes. The two draws' rounds interleave.
 __device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4 &out1, float4 v1, const CellConsts &K,
                                                  uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
                                                  uint32_t cell0, uint32_t cell1)
@@ -139,10 +141,3 @@ __device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4
     out1 = loss_noise_apply(out1, v1, K, w.b);
 }
 
-// Adds the loss-noise increment evaluated at v0 to out: the six normals of one Philox4x32-10 draw
-// (loss_fields) as three complex Wiener increments w1, w2, w3 already scaled by their amplitudes.
-__device__ __forceinline__ float4 loss_noise_cell(float4 out, float4 v0, const CellConsts &K, uint32_t k0,
-                                                  uint32_t k1, uint32_t traj, uint32_t step, uint32_t cell)
-{
-    return loss_noise_apply(out, v0, K, philox4x32_10(cell, step, traj, RNG_TAG_LOSS, k0, k1));
-}
