@@ -29,8 +29,10 @@ struct GsArgs {
 
 
 // ---------------------------------------------------------------- pencil pass
+// nz = 256: bounded to 3 CTAs (24 warps) per SM, 80 registers with a 60-byte spill; measured 4 % faster
+// over a batched ground-state loop than 2 CTAs at 99 registers
 template <int NZ>
-__global__ void __launch_bounds__(NZ) k_gs_pencil(float2 *__restrict__ state, int nx, int lx, int ny, int cells,
+__global__ void __launch_bounds__(NZ, (NZ == 256 ? 3 : 1)) k_gs_pencil(float2 *__restrict__ state, int nx, int lx, int ny, int cells,
                                                   int tiles, const GroupParamsF *__restrict__ gp,
                                                   const GsParamsF *__restrict__ gs, const int *__restrict__ tgroup,
                                                   const float2 *__restrict__ tw_g, GsArgs a,
