@@ -352,15 +352,21 @@ __global__ void k_state_sums(const float4 *__restrict__ state, int cells, int bl
     const int chunk = (cells + blocks - 1) / blocks;
     const int i0 = b * chunk, i1 = min(cells, i0 + chunk);
     const float4 *p = state + (size_t)traj * cells;
-    KVec<4> acc;
+    // plain FP64 sums over a thread's few dozen cells (rounding ~1e-15 relative), compensated across threads
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const float4 u = p[i];
         const double ax = u.x, ay = u.y, bx = u.z, by = u.w;
-        acc.v[0].add(ax * ax + ay * ay);
-        acc.v[1].add(bx * bx + by * by);
-        acc.v[2].add(ax * bx + ay * by);
-        acc.v[3].add(ax * by - ay * bx);
+        s0 = fma(ax, ax, fma(ay, ay, s0));
+        s1 = fma(bx, bx, fma(by, by, s1));
+        s2 = fma(ax, bx, fma(ay, by, s2));
+        s3 = fma(ax, by, fma(-ay, bx, s3));
     }
+    KVec<4> acc;
+    acc.v[0].add(s0);
+    acc.v[1].add(s1);
+    acc.v[2].add(s2);
+    acc.v[3].add(s3);
     KVec<4> r = block_reduce<4>(acc);
     if (threadIdx.x == 0)
         for (int k = 0; k < 4; ++k) part[(size_t)blockIdx.x * 4 + k] = r.v[k].value() * scale;

@@ -404,7 +404,7 @@ bec_status batched_moments_stored(bec_ctx *ctx)
 {
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
-        const int blocks = std::max(1, std::min({64, c.geom.cells / 4096, c.geom.nz}));
+        const int blocks = std::max(1, std::min({16, c.geom.cells / 16384, c.geom.nz}));
         const double inv = 1.0 / ((double)c.geom.nx * (double)c.geom.ny);
         fp32_state_sums(c.state, c.geom.cells, c.geom.n_traj, blocks, inv * inv, c.obs_partial, ctx->stream);
         CKL();
