@@ -94,6 +94,7 @@ struct bec_ctx {
     int max_cells = 0, max_nz = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_h2d = nullptr;        // after an init call's copies from the caller's host arrays
     std::string err;
     long long step = 0;         // steps since initialisation (Philox counter)
     long long evo_steps = 0;    // steps since bec_start_evolution
@@ -728,6 +729,7 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BEC_ERR_CUDA);
     cudaEventCreate(&ctx->ev0);
     cudaEventCreate(&ctx->ev1);
+    cudaEventCreateWithFlags(&ctx->ev_h2d, cudaEventDisableTiming);
 
     // trajectory numbering: classes in first-appearance order, groups in order within a class
     if (path == BEC_PATH_FP32_BATCHED) {
@@ -849,6 +851,7 @@ void bec_destroy(bec_ctx *ctx)
     for (auto &gr : ctx->groups)
         if (gr.gs_dev) { /* owned through allocs */ }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev_h2d) cudaEventDestroy(ctx->ev_h2d);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1454,6 +1457,7 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
     if (ctx->path == BEC_PATH_FP64_PLAIN) {
         double2 *gs = ctx->scratch_a, *nz = nullptr;
         CKC(cudaMemcpyAsync(gs, psi_gs, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        CKC(cudaEventRecord(ctx->ev_h2d, s));
         if (noise) {
             void *p = nullptr;
             CKC(cudaMalloc(&p, sizeof(double2) * 2 * (size_t)cells * ne));
@@ -1481,6 +1485,7 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
         for (int g = 0; g < group; ++g) off += sizeof(double2) * (size_t)ctx->groups[g].gd.cells;
         gr.gs_dev = reinterpret_cast<double2 *>(ctx->gs_stage + off);
         CKC(cudaMemcpyAsync(gr.gs_dev, psi_gs, sizeof(double2) * cells, cudaMemcpyHostToDevice, s));
+        CKC(cudaEventRecord(ctx->ev_h2d, s));
         float2 *nz = nullptr;
         if (noise) {
             std::vector<float2> h((size_t)2 * cells * ne);
@@ -1507,6 +1512,8 @@ bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, con
     }
     gr.initialised = true;
     ctx->last_launches = g_launches - l0;
+    // the caller may reuse psi_gs once this returns: wait for its copy (the kernels behind it keep running)
+    CKC(cudaEventSynchronize(ctx->ev_h2d));
     return BEC_OK;
 }
 
@@ -1568,6 +1575,7 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
         CKC(cudaMemcpyAsync(ctx->d_gs_ptrs, tab.data(), sizeof(void *) * ng, cudaMemcpyHostToDevice, s));
         ctx->gs_ptrs_host = tab;
     }
+    CKC(cudaEventRecord(ctx->ev_h2d, s));
     // one initialisation kernel and one preparation pass per run of consecutive listed trajectories
     for (auto &c : ctx->classes) {
         std::vector<std::pair<int, int>> runs;    // (first local trajectory, count)
@@ -1595,6 +1603,8 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
     }
     for (int i = 0; i < n; ++i) ctx->groups[groups[i]].initialised = true;
     ctx->last_launches = g_launches - l0;
+    // the caller may reuse psi_gs once this returns: wait for the copies (the kernels behind them keep running)
+    CKC(cudaEventSynchronize(ctx->ev_h2d));
     return BEC_OK;
 }
 

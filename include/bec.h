@@ -235,7 +235,8 @@ bec_status bec_warmstart_set_basis(bec_ctx *ctx, int32_t nvx, int32_t nvy, int32
  *   a = psi_gs + Va * eta_a / sqrt(dV),  b = Vb * eta_b / sqrt(dV),
  * eta complex normal with <|eta|^2> = 1/2. noise == NULL draws eta from
  * Philox4x32-10 keyed by (seed, trajectory); otherwise noise holds
- * ne * 2 * cells interleaved complex values laid out [traj][a|b][cell]. */
+ * ne * 2 * cells interleaved complex values laid out [traj][a|b][cell]. Returns once psi_gs and
+ * noise have been copied to the device (the caller may reuse them); the kernels run on. */
 bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise);
 
 /* Host element types of bec_init_groups' ground states */
@@ -249,7 +250,8 @@ enum { BEC_HOST_C128 = 0, BEC_HOST_C64 = 1 };
  * arrays lie back to back in memory in one transfer), then launches one
  * initialisation kernel and one preparation pass per run of consecutive trajectories of a grid
  * class, not one pair per group. The plain path initialises group by group. BEC_ERR_INVALID_ARG
- * for an index out of range, a repeated group, a NULL pointer or an unknown host_type.
+ * for an index out of range, a repeated group, a NULL pointer or an unknown host_type. Returns once the
+ * ground states have been copied to the device (the caller may reuse the arrays); the kernels run on.
  * Extends initEvolution (wigner.cu:202-218) and initializeEnsembles
  * (wigner_kernel.cu:295-317), which the reference calls once per ensemble. */
 bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const void *const *psi_gs,
