@@ -104,6 +104,8 @@ struct bec_ctx {
     double last_ms = 0.0;
     long long last_launches = 0;
     std::vector<void *> allocs;
+    size_t alloc_bytes = 0;              // bytes of the context's own device buffers
+    size_t alloc_limit = 0;              // BEC_DEVICE_BYTES_LIMIT at creation (0: none)
     std::vector<WsTable> ws_tables;      // warm-start bases installed per grid
 };
 
@@ -130,13 +132,19 @@ bec_status fail(bec_ctx *c, bec_status st, const std::string &msg)
             return fail(ctx, BEC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// A context's device buffers. With a byte limit set (BEC_DEVICE_BYTES_LIMIT), a buffer that would take the
+// context past it fails as an out-of-memory allocation without reaching the device: the host-side way to
+// exercise the out-of-memory paths.
 template <typename T>
 cudaError_t dalloc(bec_ctx *ctx, T **p, size_t n)
 {
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+    const size_t bytes = n * sizeof(T) > 0 ? n * sizeof(T) : 16;
+    if (ctx->alloc_limit && ctx->alloc_bytes + bytes > ctx->alloc_limit) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e == cudaSuccess) {
         ctx->allocs.push_back(q);
+        ctx->alloc_bytes += bytes;
         *p = static_cast<T *>(q);
     }
     return e;
@@ -708,6 +716,7 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
     }
     bec_ctx *ctx = new bec_ctx();
     ctx->path = path;
+    if (const char *lim = std::getenv("BEC_DEVICE_BYTES_LIMIT")) ctx->alloc_limit = (size_t)std::strtoull(lim, nullptr, 10);
     ctx->groups.resize(n_groups);
     for (int g = 0; g < n_groups; ++g) {
         GroupRec &gr = ctx->groups[g];
@@ -2092,6 +2101,7 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
 }
 
 int64_t bec_step_index(const bec_ctx *ctx) { return ctx ? ctx->step : -1; }
+int64_t bec_evolution_steps(const bec_ctx *ctx) { return ctx ? ctx->evo_steps : -1; }
 
 int32_t bec_step_graphs(const bec_ctx *ctx)
 {
@@ -2100,5 +2110,141 @@ int32_t bec_step_graphs(const bec_ctx *ctx)
 }
 double bec_last_device_ms(const bec_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
 int64_t bec_last_launch_count(const bec_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+// ---------------------------------------------------------------- checkpoint / resume
+namespace {
+constexpr uint64_t kCkptMagic = 0x3154504b43454221ull;   // "!BECKPT1" little-endian
+constexpr int32_t kCkptVersion = 1;
+
+struct CkptHeader {
+    uint64_t magic;
+    int32_t version, path, n_groups, pending;
+    int64_t n_traj, step, evo_steps, payload;
+    int32_t has_pulse, pad;
+    double pulse[8];             // pending pulse matrix, row-major (re, im)
+};
+
+struct CkptGroup {
+    int32_t nvx, nvy, nvz, ne;
+    uint64_t seed;
+};
+
+size_t ckpt_payload(const bec_ctx *ctx)
+{
+    size_t n = 0;
+    if (ctx->path == BEC_PATH_FP64_PLAIN)
+        for (auto &gr : ctx->groups) n += 2 * sizeof(double2) * (size_t)gr.p.ne * gr.d.cells;
+    else
+        for (auto &c : ctx->classes) n += sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
+    return n;
+}
+
+size_t ckpt_bytes(const bec_ctx *ctx)
+{
+    return sizeof(CkptHeader) + sizeof(CkptGroup) * ctx->groups.size() + ckpt_payload(ctx);
+}
+} // namespace
+
+int64_t bec_checkpoint_bytes(const bec_ctx *ctx) { return ctx ? (int64_t)ckpt_bytes(ctx) : 0; }
+
+bec_status bec_checkpoint_save(bec_ctx *ctx, void *buf, int64_t bytes)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!buf || bytes < (int64_t)ckpt_bytes(ctx)) return fail(ctx, BEC_ERR_INVALID_ARG, "checkpoint buffer too small");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    char *p = static_cast<char *>(buf);
+    CkptHeader h{};
+    h.magic = kCkptMagic;
+    h.version = kCkptVersion;
+    h.path = ctx->path;
+    h.n_groups = (int32_t)ctx->groups.size();
+    h.pending = ctx->pending ? 1 : 0;
+    h.n_traj = ctx->n_traj;
+    h.step = ctx->step;
+    h.evo_steps = ctx->evo_steps;
+    h.payload = (int64_t)ckpt_payload(ctx);
+    h.has_pulse = ctx->has_pulse ? 1 : 0;
+    for (int i = 0; i < 4; ++i) { h.pulse[2 * i] = ctx->pulse[i].x; h.pulse[2 * i + 1] = ctx->pulse[i].y; }
+    std::memcpy(p, &h, sizeof h);
+    p += sizeof h;
+    for (auto &gr : ctx->groups) {
+        CkptGroup g{gr.d.nvx, gr.d.nvy, gr.d.nvz, gr.p.ne, gr.p.seed};
+        std::memcpy(p, &g, sizeof g);
+        p += sizeof g;
+    }
+    // the stored device representation, bit for bit (the batched path's pending half kick and pulse stay
+    // pending, so a resumed run merges them into its next pencil pass exactly as this one would)
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        for (auto &gr : ctx->groups) {
+            const size_t n = sizeof(double2) * (size_t)gr.p.ne * gr.d.cells;
+            CKC(cudaMemcpyAsync(p, gr.a, n, cudaMemcpyDeviceToHost, ctx->stream));
+            CKC(cudaMemcpyAsync(p + n, gr.b, n, cudaMemcpyDeviceToHost, ctx->stream));
+            p += 2 * n;
+        }
+    } else {
+        for (auto &c : ctx->classes) {
+            const size_t n = sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
+            if (n) CKC(cudaMemcpyAsync(p, c.state, n, cudaMemcpyDeviceToHost, ctx->stream));
+            p += n;
+        }
+    }
+    CKC(cudaStreamSynchronize(ctx->stream));
+    return BEC_OK;
+}
+
+bec_status bec_checkpoint_load(bec_ctx *ctx, const void *buf, int64_t bytes)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!buf || bytes < (int64_t)sizeof(CkptHeader)) return fail(ctx, BEC_ERR_INVALID_ARG, "checkpoint too short");
+    const char *p = static_cast<const char *>(buf);
+    CkptHeader h;
+    std::memcpy(&h, p, sizeof h);
+    p += sizeof h;
+    if (h.magic != kCkptMagic || h.version != kCkptVersion)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "not a checkpoint of this library");
+    if (h.path != ctx->path || h.n_groups != (int32_t)ctx->groups.size() || h.n_traj != ctx->n_traj ||
+        h.payload != (int64_t)ckpt_payload(ctx) || bytes < (int64_t)ckpt_bytes(ctx) || h.step < 0 || h.evo_steps < 0)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "checkpoint of a different context layout");
+    for (auto &gr : ctx->groups) {
+        CkptGroup g;
+        std::memcpy(&g, p, sizeof g);
+        p += sizeof g;
+        if (g.nvx != gr.d.nvx || g.nvy != gr.d.nvy || g.nvz != gr.d.nvz || g.ne != gr.p.ne || g.seed != gr.p.seed)
+            return fail(ctx, BEC_ERR_INVALID_ARG, "checkpoint group differs in grid, trajectories or seed");
+    }
+    if (ctx->path == BEC_PATH_FP64_PLAIN) {
+        for (auto &gr : ctx->groups) {
+            const size_t n = sizeof(double2) * (size_t)gr.p.ne * gr.d.cells;
+            CKC(cudaMemcpyAsync(gr.a, p, n, cudaMemcpyHostToDevice, ctx->stream));
+            CKC(cudaMemcpyAsync(gr.b, p + n, n, cudaMemcpyHostToDevice, ctx->stream));
+            p += 2 * n;
+        }
+    } else {
+        for (auto &c : ctx->classes) {
+            const size_t n = sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
+            if (n) CKC(cudaMemcpyAsync(c.state, p, n, cudaMemcpyHostToDevice, ctx->stream));
+            p += n;
+        }
+    }
+    CKC(cudaStreamSynchronize(ctx->stream));
+    ctx->step = h.step;
+    ctx->evo_steps = h.evo_steps;
+    ctx->pending = h.pending != 0;
+    ctx->has_pulse = h.has_pulse != 0;
+    for (int i = 0; i < 4; ++i) ctx->pulse[i] = make_double2(h.pulse[2 * i], h.pulse[2 * i + 1]);
+    for (auto &gr : ctx->groups) gr.initialised = true;
+    return BEC_OK;
+}
+
+bec_status bec_set_step_index(bec_ctx *ctx, int64_t step, int64_t evo_steps)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (step < 0 || evo_steps < 0 || step > 0xFFFFFFFFll)
+        return fail(ctx, BEC_ERR_INVALID_ARG, "step index out of range");
+    ctx->step = step;
+    ctx->evo_steps = evo_steps;
+    return BEC_OK;
+}
 
 } // extern "C"

@@ -12,11 +12,11 @@
 //
 // The scratch array below is a file-scope __device__ symbol: every GPU that
 // loads this library holds its 64 KiB until the process exits. In host code
-// its name is only a host-side stand-in, not a device address, so the device
-// address is looked up with cudaGetSymbolAddress once per device (on the first
-// call with that device current) and passed to the kernels.
-#include <mutex>
-
+// its name is only a host-side stand-in, not a device address, so every call
+// looks up its device address in the current context with cudaGetSymbolAddress
+// (a host-side lookup that allocates nothing) and passes it to the kernels. A
+// fresh lookup per call stays right after a device reset, which may load the
+// module at another address, and under a non-primary context.
 #include "engine.h"
 #include "reduce.cuh"
 
@@ -24,13 +24,9 @@ namespace {
 
 constexpr int kNoallocMaxBlocks = 1024;                 // partial sums kept per call
 constexpr int kNoallocSums = 4;                         // |a|^2, |b|^2, Re and Im of conj(a) b
-constexpr int kNoallocMaxDevices = 64;
 
 // Partial (sum, carry) pairs of the first reduction stage: 1024 blocks x 4 sums x 2 doubles = 64 KiB.
 static __device__ __align__(256) double g_noalloc_partials[kNoallocMaxBlocks * kNoallocSums * 2];
-
-double *g_partials_addr[kNoallocMaxDevices] = {};
-std::mutex g_partials_mutex;
 
 // psi: [traj][a|b][cell] interleaved complex doubles (x-space)
 struct F_moments {
@@ -64,21 +60,13 @@ __global__ void k_noalloc_finish(const double *part, int nparts, double dV, doub
     }
 }
 
-// Device address of the scratch array on the current device (looked up once per device).
+// Device address of the scratch array in the current context.
 cudaError_t partials_on_current_device(double **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_partials_mutex);
-    if (!g_partials_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess) return e;
-        g_partials_addr[dev] = static_cast<double *>(p);
-    }
-    *out = g_partials_addr[dev];
+    *out = static_cast<double *>(p);
     return cudaSuccess;
 }
 

@@ -24,6 +24,9 @@
 
 namespace {
 
+constexpr int kMaxGridY = 65535;   // largest gridDim.y of a launch
+
+
 constexpr int kRad = 16, kAng = 4, kBasis = kRad * kAng;
 
 __device__ __constant__ float c_rc[kRad];   // radial centres
@@ -279,6 +282,7 @@ cudaError_t warmstart_table_init(WsTable &t, const float *host_basis, cudaStream
 cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, const WsTable *tab, double *coef_out,
                               float *profile_out, cudaStream_t s)
 {
+    if (n < 1 || n > kMaxGridY) return cudaErrorInvalidValue;   // n is the launch's grid y
     cudaError_t e = set_consts(s);
     if (e) return e;
     const WsGeom g = geom_dims(d[0].nvx, d[0].nvy, d[0].nvz);
@@ -298,6 +302,11 @@ cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, co
     if (tab) k_ws_project<true><<<grid, 256, 0, s>>>(psi, n, g, damp, tab->d_basis, tab->nb, rhs, dprof);
     else k_ws_project<false><<<grid, 256, 0, s>>>(psi, n, g, damp, nullptr, kBasis, rhs, dprof);
     g_launches++;
+    if ((e = cudaGetLastError())) {           // nothing solved from a projection that did not run
+        cudaStreamSynchronize(s);
+        cudaFree(damp); cudaFree(rhs); cudaFree(dprof);
+        return e;
+    }
     std::vector<double> hr((size_t)n * kBasis);
     cudaMemcpyAsync(hr.data(), rhs, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost, s);
     if (profile_out)
@@ -322,6 +331,7 @@ cudaError_t warmstart_project(const float2 *psi, int n, const bec_derived *d, co
 cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, const WsTable *tab, float2 *psi_out,
                             cudaStream_t s)
 {
+    if (n < 1 || n > kMaxGridY) return cudaErrorInvalidValue;   // n is the launch's grid y
     cudaError_t e = set_consts(s);
     if (e) return e;
     const WsGeom g = geom_dims(d[0].nvx, d[0].nvy, d[0].nvz);
@@ -337,7 +347,8 @@ cudaError_t warmstart_synth(const double *coef, int n, const bec_derived *d, con
     if (tab) k_ws_synth<true><<<grid, 256, 0, s>>>(psi_out, n, g, damp, dc, tab->d_basis, tab->nb);
     else k_ws_synth<false><<<grid, 256, 0, s>>>(psi_out, n, g, damp, dc, nullptr, kBasis);
     g_launches++;
+    const cudaError_t el = cudaGetLastError();
     e = cudaStreamSynchronize(s);
     cudaFree(damp); cudaFree(dc);
-    return e ? e : cudaGetLastError();
+    return el ? el : e;
 }

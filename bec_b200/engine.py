@@ -49,6 +49,11 @@ SIGNATURES = {
     "bec_get_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "bec_set_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "bec_step_index": (C.c_int64, [C.c_void_p]),
+    "bec_evolution_steps": (C.c_int64, [C.c_void_p]),
+    "bec_set_step_index": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
+    "bec_checkpoint_bytes": (C.c_int64, [C.c_void_p]),
+    "bec_checkpoint_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "bec_checkpoint_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "bec_step_graphs": (C.c_int32, [C.c_void_p]),
     "bec_last_device_ms": (C.c_double, [C.c_void_p]),
     "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
@@ -161,6 +166,26 @@ class Engine:
     @property
     def step_index(self):
         return int(lib().bec_step_index(self._h))
+
+    @property
+    def evolution_steps(self):
+        return int(lib().bec_evolution_steps(self._h))
+
+    def set_step_index(self, step, evolution_steps):
+        """Continues the Philox loss-noise stream of a saved run (after set_state in a fresh context)."""
+        self._check(lib().bec_set_step_index(self._h, int(step), int(evolution_steps)), "bec_set_step_index")
+
+    def checkpoint(self):
+        """The whole evolution state, bit for bit, as bytes (bec_checkpoint_save)."""
+        n = int(lib().bec_checkpoint_bytes(self._h))
+        buf = C.create_string_buffer(n)
+        self._check(lib().bec_checkpoint_save(self._h, buf, n), "bec_checkpoint_save")
+        return buf.raw
+
+    def restore(self, blob):
+        """Loads a checkpoint of a context with the same groups and path (bec_checkpoint_load)."""
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        self._check(lib().bec_checkpoint_load(self._h, buf, len(blob)), "bec_checkpoint_load")
 
     @property
     def step_graphs(self):

@@ -26,9 +26,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # ncu: DRAM bytes (read + write) of one launch divided by its trajectory count,
-# from captures of a 64-trajectory 32x32x256 class (profiles/plane_32x32x256.md,
-# profiles/pencil_32x32x256.md); traffic scales with the trajectories a launch
-# processes. Algorithmic: 32 B x 262144 cells = 8.39 MB per trajectory.
+# from captures of a 64-trajectory 32x32x256 class; traffic scales with the
+# trajectories a launch processes. Algorithmic: 32 B x 262144 cells = 8.39 MB
+# per trajectory.
 NCU_TRAFFIC_PER_TRAJ = {
     "plane_32x32x256": (268.500224e6 + 210.539776e6) / 64,
     "pencil_32x32x256": (268.492800e6 + 209.569280e6) / 64,

@@ -28,14 +28,14 @@
 extern "C" {
 #endif
 
-#define BEC_ABI_VERSION 2
+#define BEC_ABI_VERSION 3
 
 typedef enum bec_status {
     BEC_OK = 0,
     BEC_ERR_INVALID_ARG = 1,      /* bad pointer, size or parameter value */
     BEC_ERR_UNSUPPORTED_GRID = 2, /* grid not a supported power-of-two shape */
     BEC_ERR_CUDA = 3,             /* a CUDA runtime call failed; see bec_last_error */
-    BEC_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed */
+    BEC_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed (or would pass BEC_DEVICE_BYTES_LIMIT) */
     BEC_ERR_STATE = 5,            /* call out of order (e.g. evolve before init) */
     BEC_ERR_NUMERICAL = 6,        /* NaN/Inf or norm blow-up detected in a reduction */
     BEC_ERR_NO_DEVICE = 7,        /* no CUDA device visible */
@@ -182,6 +182,9 @@ bec_status bec_derive_params(const bec_params *p, bec_derived *out);
 /* ---- context ---------------------------------------------------------- */
 
 /* Creates a context holding n_groups ensembles on the current CUDA device.
+ * If the environment sets BEC_DEVICE_BYTES_LIMIT (bytes), the context's own device buffers may
+ * not exceed it: creation then fails with BEC_ERR_OUT_OF_MEMORY before the device is asked,
+ * which exercises the out-of-memory paths without filling a GPU.
  * Replaces initConstants + initWaveVectors + EvolutionState::init
  * (wigner_kernel.cu:395-399, :25-55; defines.h:157-184). */
 bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, bec_ctx **out);
@@ -324,7 +327,28 @@ bec_status bec_phase_scan(const bec_ctx *ctx, int32_t group, const bec_moments *
  * interleaved complex (2 * cells complex values). */
 bec_status bec_get_state(bec_ctx *ctx, int32_t group, int32_t traj, double *ab_out);
 bec_status bec_set_state(bec_ctx *ctx, int32_t group, int32_t traj, const double *ab_in);
+/* Steps taken since initialisation: the step counter of the Philox loss-noise draws. */
 int64_t bec_step_index(const bec_ctx *ctx);
+/* Steps taken since bec_start_evolution (moments report t = this count times dt_evo). */
+int64_t bec_evolution_steps(const bec_ctx *ctx);
+/* Sets both counters, e.g. after bec_set_state in a fresh context resuming a saved run, so
+ * that its loss noise continues the saved run's Philox stream (step <= 2^32 - 1). The
+ * reference has no counterpart: its noise came from the host rand() seeded by the time
+ * (wigner.cu:210). */
+bec_status bec_set_step_index(bec_ctx *ctx, int64_t step, int64_t evo_steps);
+
+/*
+ * Checkpoints: the stored device representation of every trajectory, bit for bit, with the
+ * step counters and any pending half kick or pulse of the batched path, so that a context
+ * created with the same groups and path resumes the run bit-identically
+ * (bec_checkpoint_load, then bec_evolve / bec_run). No counterpart in the reference, which
+ * keeps its ground state in host memory and has its state dumps commented out
+ * (wigner.cpp:335-362). bytes must be at least bec_checkpoint_bytes(ctx); the load checks
+ * grids, trajectory counts, seeds and path against the context (BEC_ERR_INVALID_ARG).
+ */
+int64_t bec_checkpoint_bytes(const bec_ctx *ctx);
+bec_status bec_checkpoint_save(bec_ctx *ctx, void *buf, int64_t bytes);
+bec_status bec_checkpoint_load(bec_ctx *ctx, const void *buf, int64_t bytes);
 
 /* Batched path: steady steps (no pulse or sample due) replay CUDA graphs captured once per context
  * (8 steps and 1 step; set BEC_CUDA_GRAPHS=0 in the environment before bec_create to launch them one by
@@ -391,16 +415,19 @@ bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_
  *   d_psi: ne * 2 * cells interleaved complex doubles laid out [traj][a|b][cell];
  *   d_out: 4 doubles of device memory receiving sum |a|^2 dV, sum |b|^2 dV and
  *          the real and imaginary parts of sum conj(a) b dV over all trajectories;
- *   stream: a cudaStream_t, or NULL for the default stream. The call only
- *          enqueues work: synchronise the stream before reading d_out.
+ *   stream: a cudaStream_t of the current device, or NULL for the default
+ *          stream. The call only enqueues work: synchronise the stream before
+ *          reading d_out.
  * No counterpart in the reference. It exists for callers that cannot let a
  * library call cudaMalloc: hosts whose device memory all comes from their own
  * pool, and loops that must never block on an allocation (cudaMalloc and
  * cudaFree synchronise the device and can fail mid-run). It allocates nothing:
  * the reduction's partial sums live in a fixed 64 KiB array that is part of the
  * library image (every GPU that loads the library holds it until the process
- * exits). The first call on a device looks up that array's device address, so
- * make one call on each device before capturing any stream. All calls share
+ * exits). Every call looks up that array's device address in the current
+ * context (no allocation); the first call on a device also loads the library's
+ * device code there, so make one call on each device before capturing any
+ * stream. All calls share
  * the array: calls that overlap on the GPU (different streams, or several host
  * threads) race and must be serialised by the caller; each call rewrites every
  * partial sum it reads, so nothing carries over from the previous call.

@@ -10,7 +10,7 @@
    stopping rule (wigner.cu:148-156), one equilibration step, pi/2, then
    15000 steps of 40 us sampled every 250 steps.
 
-    python tests/golden/make_golden.py [--reference-data DIR]
+    python tests/golden/make_golden.py --reference-data <reference checkout>/data
 """
 import argparse
 import ast
@@ -27,7 +27,8 @@ sys.path.insert(0, ROOT)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-data", default="/root/reference/data")
+    ap.add_argument("--reference-data", required=True,
+                    help="the reference's data/ directory (holds gpu_sp_30k.yaml and gpu_sp_30k_4ens.yaml)")
     a = ap.parse_args()
     import yaml
     from bec_b200 import observables as OBS

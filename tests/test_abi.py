@@ -32,7 +32,7 @@ def test_library_exports_every_declared_function():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(E.SIGNATURES), "ctypes signature table out of date"
-    assert lib.bec_abi_version() == 2
+    assert lib.bec_abi_version() == 3
 
 
 def test_struct_layout_matches_c_compiler():

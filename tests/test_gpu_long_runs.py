@@ -1,0 +1,130 @@
+"""Long runs of the batched FP32 path against committed FP64 oracle runs of the same seeds.
+
+Fixtures (tests/golden/make_long_runs.py, the CPU FP64 oracle):
+  * the 3D truncated-Wigner ensemble: 16x16x128, N = 30000, 4 trajectories, Philox vacuum and loss
+    noise, pi/2, then 200 ms (5000 steps of 40 us), sampled every 250 steps;
+  * the Ramsey / spin-echo sequence at 4 trajectories: 32x32x256, N = 70000, pi/2, 0.5 s, pi, 0.5 s
+    (25000 steps), sampled every 500 steps, then the final pi/2 about 50 axis angles.
+The ground state is the FP64 plain path's (2000 fixed imaginary-time steps, within 1e-10 of the
+oracle's), so both runs start from the same input. Per sample the test compares each observable of
+the reference's (wigner.cu:257-303, :363-369): per-trajectory populations N1, N2, ensemble visibility,
+phase arg <psi1|psi2>, the per-trajectory phase spread (phase noise) and the axial ratio
+(a - b)/(a + b)(z) after a pi/2; and, after the spin echo, the populations of the final pi/2 at the
+50 phase points against the oracle's literal halfPiRotate + reduce. The measured worst errors are
+stated in the design notes; the bounds below leave them a margin.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from bec_b200 import observables as OBS
+from bec_b200._abi import BEC_GS_FIXED_STEPS
+from bec_b200.configs import copy_params, ensemble_16x16x128, spin_echo_32x32x256
+from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
+from parity_util import record
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _load(name):
+    z = np.load(os.path.join(HERE, name))
+    meta = json.loads(str(z["meta"]))
+    return meta, {k: z[k] for k in z.files if k != "meta"}
+
+
+def _phase_spread(traj):
+    """circular standard deviation of the per-trajectory phases arg s_t"""
+    ph = np.arctan2(traj[:, 4], traj[:, 3])
+    r = np.abs(np.exp(1j * ph).mean())
+    return float(np.sqrt(max(-2.0 * np.log(max(r, 1e-300)), 0.0)))
+
+
+def _engine_run(p, meta):
+    gs_eng = Engine([copy_params(p, ne=1)], path=BEC_PATH_FP64_PLAIN)
+    gs, rep = gs_eng.ground_state(0, mode=BEC_GS_FIXED_STEPS, max_steps=meta["gs_steps"])
+    gs_eng.close()
+    eng = Engine([p], path=BEC_PATH_FP32_BATCHED)
+    eng.init_group(0, gs)
+    eng.start_evolution()
+    every, steps, pi_step = meta["sample_every"], meta["steps"], meta["pi_pulse_step"]
+    mom, traj, axial = [], [], []
+    done = 0
+    # run sample by sample so that per-trajectory moments are read at every sample; axial samples end
+    # their step with the observing pass, moments-only samples read the stored state
+    while done < steps:
+        k = every
+        want_axial = (done + k) % meta["axial_every"] == 0
+        pulse_at = pi_step - done if done < pi_step <= done + k else -1
+        out = eng.run(k, sample_every=k, pi_pulse_step=pulse_at, axial=want_axial)
+        if want_axial:
+            m, ax = out
+            axial.append(ax[0][-1])
+        else:
+            m = out
+        mom.append(m[-1, 0])
+        traj.append(eng.traj_moments())
+        done += k
+    return eng, rep, np.array(mom), np.array(traj), np.array(axial)
+
+
+def _compare(name, p, meta, fx, eng, mom, traj, axial):
+    d = eng.derived[0]
+    mo, to, axo = fx["moments"], fx["traj_moments"], fx["axial"]
+    assert mom.shape == mo.shape and traj.shape == to.shape and axial.shape == axo.shape
+    np.testing.assert_allclose(mom[:, 0], mo[:, 0], rtol=1e-12)
+    n1e, n2e = OBS.populations(mom.T, d, p.ne)
+    n1o, n2o = OBS.populations(mo.T, d, p.ne)
+    err = dict(
+        N1=float(np.max(np.abs(n1e - n1o) / n1o.max())),
+        N2=float(np.max(np.abs(n2e - n2o) / max(n1o.max(), n2o.max()))),
+        visibility=float(max(abs(OBS.visibility(a, d, p.ne) - OBS.visibility(b, d, p.ne)) for a, b in zip(mom, mo))),
+        phase=float(max(abs(np.angle(np.exp(1j * (OBS.phase(a) - OBS.phase(b))))) for a, b in zip(mom, mo))),
+        phase_noise=float(max(abs(_phase_spread(a) - _phase_spread(b)) for a, b in zip(traj, to))),
+        traj_population=float(np.max(np.abs(traj[:, :, 1:3] - to[:, :, 1:3]) / to[:, :, 1:3].max())),
+    )
+    sub = p.ne * d.nvx * d.nvy * d.V / 2.0
+    worst_ratio = 0.0
+    for ae, ao in zip(axial, axo):
+        tot = ao[:, 0] + ao[:, 1] - 2 * sub
+        keep = np.abs(tot) > 0.05 * np.abs(tot).max()
+        worst_ratio = max(worst_ratio, float(np.abs(OBS.axial_ratio(ae, d, p.ne) - OBS.axial_ratio(ao, d, p.ne))[keep].max()))
+    err["axial_ratio"] = worst_ratio
+    record(name, **err)
+    return err
+
+
+def test_ensemble_16x16x128_200ms():
+    meta, fx = _load("ensemble_16x16x128_5000.npz")
+    p = ensemble_16x16x128(ne=4, seed=0)
+    eng, rep, mom, traj, axial = _engine_run(p, meta)
+    assert rep.mu == pytest.approx(float(fx["gs_mu"]), rel=1e-10)
+    err = _compare("long_ensemble_16x16x128", p, meta, fx, eng, mom, traj, axial)
+    assert err["visibility"] < 1e-3
+    assert err["N1"] < 1e-3 and err["N2"] < 1e-3
+    assert err["phase"] < 1e-2
+    assert err["phase_noise"] < 1e-2
+    assert err["axial_ratio"] < 1e-2
+
+
+def test_spin_echo_32x32x256_one_second():
+    meta, fx = _load("spin_echo_32x32x256_4traj.npz")
+    p = spin_echo_32x32x256(ne=4, seed=4)
+    eng, rep, mom, traj, axial = _engine_run(p, meta)
+    assert rep.mu == pytest.approx(float(fx["gs_mu"]), rel=1e-10)
+    err = _compare("long_spin_echo_32x32x256", p, meta, fx, eng, mom, traj, axial)
+    # final pi/2 at 50 phase points: closed form from the FP32 run's moments against the oracle's literal
+    # rotation of its own state
+    scan = eng.phase_scan(0, mom[-1], fx["alpha"]) * p.ne
+    rot = fx["rotated_sums"]
+    err_scan = float(np.max(np.abs(scan - rot)) / np.abs(rot).max())
+    record("long_spin_echo_phase_scan", phase_scan=err_scan)
+    assert err["visibility"] < 1e-3
+    assert err["N1"] < 1e-3 and err["N2"] < 1e-3
+    assert err["phase"] < 1e-2
+    assert err["phase_noise"] < 1e-2
+    assert err["axial_ratio"] < 1e-2
+    assert err_scan < 1e-3

@@ -3,9 +3,12 @@ computed without any device allocation (for callers that cannot let the
 library call cudaMalloc: hosts that own all device memory through their own
 pool, and loops that must never block on an allocation).
 
-Checked through the C ABI against bec_moments_now of a context holding the
-same states, on two calls in a row with different inputs and sizes (the
-second call runs over the scratch contents the first one left behind).
+Checked through the C ABI against an FP64 NumPy sum of the same array and
+against bec_moments_now of a context holding the same states, on calls in a
+row with different inputs and sizes: a large call whose grid-stride first
+stage is clamped to the 1024 partial sums of the scratch array, then smaller
+calls that must not pick up the partial sums the large call left behind.
+After a warm-up call, the calls leave the device's free memory unchanged.
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
 import ctypes as C
@@ -46,6 +49,12 @@ def _noalloc(psi, cells, ne, dV):
     return st, out.cpu().numpy()
 
 
+def _numpy_moments(psi, dV):
+    a, b = psi[:, 0], psi[:, 1]
+    s = (np.conj(a) * b).sum()
+    return np.array([(np.abs(a) ** 2).sum(), (np.abs(b) ** 2).sum(), s.real, s.imag]) * dV
+
+
 def test_noalloc_moments_match_context_moments_twice():
     cases = [((16, 16, 128), 3, 1), ((8, 8, 64), 2, 2)]
     for grid, ne, seed in cases:
@@ -53,6 +62,40 @@ def test_noalloc_moments_match_context_moments_twice():
         st, got = _noalloc(psi, cells, ne, dV)
         assert st == BEC_OK
         np.testing.assert_allclose(got, expect[1:], rtol=TOL, atol=TOL * np.abs(expect[1:3]).max())
+        ref = _numpy_moments(psi, dV)
+        np.testing.assert_allclose(got, ref, rtol=TOL, atol=TOL * np.abs(ref[:2]).max())
+
+
+def test_noalloc_clamped_grid_then_smaller_calls_allocate_nothing():
+    import torch
+    rng = np.random.default_rng(7)
+    # 32 x 32 x 256 cells x 2 trajectories: 524,288 cells per call, twice the 262,144 that 1024 blocks of
+    # 256 threads cover in one pass, so the first stage loops over its grid stride
+    big = (rng.standard_normal((2, 2, 262144)) + 1j * rng.standard_normal((2, 2, 262144))) * 0.5
+    small = (rng.standard_normal((1, 2, 4096)) + 1j * rng.standard_normal((1, 2, 4096))) * 2.0
+    mid = (rng.standard_normal((3, 2, 32768)) + 1j * rng.standard_normal((3, 2, 32768)))
+    dV = 0.37
+    d_big = torch.from_numpy(big.view(np.float64).reshape(-1).copy()).cuda()
+    d_small = torch.from_numpy(small.view(np.float64).reshape(-1).copy()).cuda()
+    d_mid = torch.from_numpy(mid.view(np.float64).reshape(-1).copy()).cuda()
+    out = torch.empty(4, dtype=torch.float64, device="cuda")
+    L = lib()
+
+    def call(d, cells, ne):
+        out.fill_(float("nan"))
+        st = L.bec_moments_device_noalloc(C.c_void_p(d.data_ptr()), cells, ne, dV, C.c_void_p(out.data_ptr()), None)
+        torch.cuda.synchronize()
+        return st, out.cpu().numpy()
+
+    assert call(d_small, 4096, 1)[0] == BEC_OK           # warm-up: loads the device code
+    free0 = torch.cuda.mem_get_info()[0]
+    for d, psi, cells, ne in ((d_big, big, 262144, 2), (d_small, small, 4096, 1), (d_mid, mid, 32768, 3),
+                              (d_big, big, 262144, 2), (d_small, small, 4096, 1)):
+        st, got = call(d, cells, ne)
+        assert st == BEC_OK
+        ref = _numpy_moments(psi, dV)
+        np.testing.assert_allclose(got, ref, rtol=TOL, atol=TOL * np.abs(ref[:2]).max())
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 def test_noalloc_rejects_bad_sizes():
