@@ -252,16 +252,11 @@ __global__ void __launch_bounds__(kThreads) k_zpass(float4 *state, ClassGeom c, 
     for (int idx = threadIdx.x; idx < npen * n; idx += blockDim.x) {
         const int pen = idx / n, z = idx - pen * n;
         const int xl = pen % tx, yl = pen / tx;
-        const float kx = getk<float>(x0 + xl, P.dkx, c.nx);
-        const float ky = (c.ny > 1) ? getk<float>(y0 + yl, P.dky, c.ny) : 0.0f;
-        const float kz = getk<float>(z, P.dkz, n);
-        const float k2h = (kx * kx + ky * ky + kz * kz) * 0.5f;
+        const int ix = kidx(x0 + xl, c.nx), iy = c.ny > 1 ? kidx(y0 + yl, c.ny) : 0, iz = kidx(z, n);
+        const double k2h = P.kin_x * (double)(ix * ix) + P.kin_y * (double)(iy * iy) + P.kin_z * (double)(iz * iz);
         float4 v = pscale(buf[idx], za.observe ? za.scale : za.scale * za.out_scale);
-        if (kick_first != 0.0f) {
-            float s, co;
-            sincosf(k2h * P.dt * kick_first, &s, &co);     // e^{+i k^2/2 dt}, wigner_kernel.cu:143-144
-            v = pmul(v, make_float2(co, s));
-        }
+        if (kick_first != 0.0f)
+            v = pmul(v, kin_phase(k2h * (double)kick_first));   // e^{+i k^2/2 dt}, wigner_kernel.cu:143-144
         if (za.has_m1) v = apply_m(za.m1, v);
         if (!za.observe && za.has_m2) v = apply_m(za.m2, v);
         buf[idx] = v;
@@ -294,13 +289,10 @@ __global__ void __launch_bounds__(kThreads) k_zpass(float4 *state, ClassGeom c, 
             float4 v = pscale(buf[idx], inv_n);
             if (za.has_m2) v = apply_m(za.m2, v);
             if (za.post != 0.0f) {
-                const float kx = getk<float>(x0 + xl, P.dkx, c.nx);
-                const float ky = (c.ny > 1) ? getk<float>(y0 + yl, P.dky, c.ny) : 0.0f;
-                const float kz = getk<float>(z, P.dkz, n);
-                const float k2h = (kx * kx + ky * ky + kz * kz) * 0.5f;
-                float s, co;
-                sincosf(k2h * P.dt * za.post, &s, &co);
-                v = pmul(v, make_float2(co, s));
+                const int ix = kidx(x0 + xl, c.nx), iy = c.ny > 1 ? kidx(y0 + yl, c.ny) : 0, iz = kidx(z, n);
+                const double k2h =
+                    P.kin_x * (double)(ix * ix) + P.kin_y * (double)(iy * iy) + P.kin_z * (double)(iz * iz);
+                v = pmul(v, kin_phase(k2h * (double)za.post));
             }
             buf[idx] = v;
         }

@@ -76,6 +76,10 @@ struct bec_ctx {
     uint32_t *d_step = nullptr;          // batched: Philox step index the plane passes read
     bool use_graphs = true;              // batched: steady steps replay captured CUDA graphs
     bool graphs_failed = false;
+    StepPlan plan;                       // batched: the fused step of the register-path classes
+    std::vector<char> fused;             // per class: 1 when its passes run in the fused step
+    int plan_mode = -2;                  // -2: not chosen yet, -1: per-pass launches, >= 0: fused candidate
+    std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
     long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
     GroupParamsF *d_gparams = nullptr;
@@ -214,6 +218,9 @@ GroupParamsF make_gf(const GeomD &g)
     f.noise = g.noise;
     f.seed_lo = (uint32_t)g.seed;
     f.seed_hi = (uint32_t)(g.seed >> 32);
+    f.kin_x = 0.5 * g.dkx * g.dkx * g.dt_evo / (2.0 * M_PI);
+    f.kin_y = g.ny > 1 ? 0.5 * g.dky * g.dky * g.dt_evo / (2.0 * M_PI) : 0.0;
+    f.kin_z = 0.5 * g.dkz * g.dkz * g.dt_evo / (2.0 * M_PI);
     return f;
 }
 
@@ -306,8 +313,10 @@ bec_status plain_step(bec_ctx *ctx, GroupRec &gr, int t)
 // ---------------------------------------------------------------- batched z pass
 // ends_step: no plane pass follows, so the pass leaves the state in the form a z pass reads
 // ev (optional): per class (start, stop) events recorded around that class's launch
+// skip_fused: leave out the classes of the fused step plan (their pencil pass runs inside it)
 bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, const double2 *m2,
-                             bool ends_step = false, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr)
+                             bool ends_step = false, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr,
+                             bool skip_fused = false)
 {
     ZPassArgs z{};
     z.pre = pre;
@@ -336,6 +345,7 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
     }
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
+        if (skip_fused && ctx->fused[&c - &ctx->classes[0]]) continue;
         bec_status st;
         z.scale = (float)(1.0 / (double)c.geom.cells);
         z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
@@ -363,15 +373,18 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
     return BEC_OK;
 }
 
-// put_step: write ctx->step into the device step scalar first (eager launches); otherwise increment
-// it (the body of a captured step graph, replayed from a known start value)
-bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr, bool put_step = true)
+// put_step: write ctx->step into the device step scalar first (eager launches; a captured step graph
+// leaves it to the step before); skip_fused: leave out the classes of the fused step plan
+bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr, bool put_step = true,
+                             bool skip_fused = false)
 {
-    if (put_step) fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
-    else fp32_inc_step(ctx->d_step, ctx->stream);
-    CKL();
+    if (put_step) {
+        fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
+        CKL();
+    }
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
+        if (skip_fused && ctx->fused[&c - &ctx->classes[0]]) continue;
         const size_t ci = &c - &ctx->classes[0];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
         if (ctx->use_fast && fp32_fast_plane_supported(c.geom)) {
@@ -386,6 +399,156 @@ bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *
         if (ev) CKC(cudaEventRecord(ev[ci].second, ctx->stream));
         CKL();
     }
+    return BEC_OK;
+}
+
+// One split step of every class, ending with its plane pass: kick fraction pre of dt before this step's half
+// kick (0.5 while the previous step's second half kick is pending), then any pending pulse. The classes of
+// the fused plan run as one launch of the fused step kernel, which advances the device step index; the
+// others launch their own passes, and without a fused plan a one-thread launch advances it. put_step writes
+// the host step index to the device first (eager steps); a captured step graph leaves it to the step before.
+bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
+{
+    if (put_step) {
+        fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
+        CKL();
+    }
+    const bool fused = ctx->plan.ready;
+    float2 mf[4];
+    const bool has_m = ctx->has_pulse;
+    if (has_m)
+        for (int i = 0; i < 4; ++i) mf[i] = make_float2((float)ctx->pulse[i].x, (float)ctx->pulse[i].y);
+    bec_status st;
+    if ((st = batched_zpass_all(ctx, pre, 0.5f, false, nullptr, false, nullptr, fused))) return st;
+    if ((st = batched_ppass_all(ctx, nullptr, false, fused))) return st;
+    if (fused) step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, pre + 0.5f, has_m ? mf : nullptr, ctx->stream);
+    else fp32_inc_step(ctx->d_step, ctx->stream);
+    CKL();
+    return BEC_OK;
+}
+
+// The fused step plan of a batched context, chosen once before its first step. BEC_STEP_PLAN in the
+// environment forces one ("unfused" for launches per pass, or a candidate number 0..4); otherwise a plan
+// cached for the same class mix on this device is reused, or the candidates are timed on a copy of the
+// state (BEC_AUTOTUNE=0 skips the timing and takes the one-wave interleave).
+bec_status ensure_plan(bec_ctx *ctx)
+{
+    if (ctx->path != BEC_PATH_FP32_BATCHED || ctx->plan_mode != -2) return BEC_OK;
+    ctx->fused.assign(ctx->classes.size(), 0);
+    const char *force = std::getenv("BEC_STEP_PLAN");
+    std::vector<ClassGeom> geoms;
+    std::vector<StepClassDev> devs;
+    std::vector<int> offs, idx;
+    if (ctx->use_fast && !(force && std::string(force) == "unfused")) {
+        for (size_t ci = 0; ci < ctx->classes.size(); ++ci) {
+            ClassRec &c = ctx->classes[ci];
+            if (c.geom.n_traj == 0 || !step_class_supported(c.geom)) continue;
+            float2 *twf;
+            bec_status st;
+            if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
+            StepClassDev d{};
+            d.state = c.state;
+            d.tgroup = c.d_tgroup;
+            d.tlocal = c.d_tlocal;
+            d.tw = twf;
+            d.nx = c.geom.nx; d.ny = c.geom.ny; d.nz = c.geom.nz; d.lx = c.geom.lx;
+            d.cells = c.geom.cells; d.tiles = c.geom.nx * c.geom.ny / 16; d.n_traj = c.geom.n_traj;
+            geoms.push_back(c.geom);
+            devs.push_back(d);
+            offs.push_back(c.traj_offset);
+            idx.push_back((int)ci);
+        }
+    }
+    if (geoms.empty()) {
+        ctx->plan_mode = -1;
+        ctx->plan_desc = "{\"plan\": \"unfused\", \"launches_per_step\": \"2 per class\"}";
+        return BEC_OK;
+    }
+    int cand = -1;
+    std::string how;
+    std::vector<double> tms(kStepCandidates, -1.0);
+    if (force && *force) {
+        cand = std::atoi(force);
+        if (cand < 0 || cand >= kStepCandidates) return fail(ctx, BEC_ERR_INVALID_ARG, "BEC_STEP_PLAN out of range");
+        how = "forced";
+    } else if ((cand = step_plan_cached(geoms)) >= 0) {
+        how = "cached";
+    } else {
+        const char *at = std::getenv("BEC_AUTOTUNE");
+        cand = 2;
+        how = "default";
+        if (!(at && at[0] == '0')) {
+            // time every candidate on a copy of the state: the copy is restored afterwards, so tuning
+            // changes nothing of the run (every candidate computes the same bits anyway)
+            size_t bytes = 0;
+            for (const ClassGeom &g : geoms) bytes += sizeof(float4) * (size_t)g.n_traj * g.cells;
+            char *save = nullptr;
+            if (cudaMalloc(&save, bytes) == cudaSuccess) {
+                size_t o = 0;
+                for (const StepClassDev &d : devs) {
+                    const size_t n = sizeof(float4) * (size_t)d.n_traj * d.cells;
+                    CKC(cudaMemcpyAsync(save + o, d.state, n, cudaMemcpyDeviceToDevice, ctx->stream));
+                    o += n;
+                }
+                bec_status st = BEC_OK;
+                double best = 1e30;
+                for (int k = 0; k < kStepCandidates && st == BEC_OK; ++k) {
+                    if (step_plan_build(ctx->plan, geoms, devs, offs, k, ctx->stream) != cudaSuccess) {
+                        st = fail(ctx, BEC_ERR_CUDA, "fused step plan");
+                        break;
+                    }
+                    fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
+                    step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, 1.0f, nullptr, ctx->stream);
+                    cudaEventRecord(ctx->ev0, ctx->stream);
+                    for (int r = 0; r < 3; ++r)
+                        step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, 1.0f, nullptr, ctx->stream);
+                    cudaEventRecord(ctx->ev1, ctx->stream);
+                    if (cudaEventSynchronize(ctx->ev1) != cudaSuccess) {
+                        st = fail(ctx, BEC_ERR_CUDA, std::string("fused step: ") + cudaGetErrorString(cudaGetLastError()));
+                        break;
+                    }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+                    tms[k] = ms / 3.0;
+                    if (tms[k] < best) { best = tms[k]; cand = k; }
+                }
+                o = 0;
+                for (const StepClassDev &d : devs) {
+                    const size_t n = sizeof(float4) * (size_t)d.n_traj * d.cells;
+                    cudaMemcpyAsync(d.state, save + o, n, cudaMemcpyDeviceToDevice, ctx->stream);
+                    o += n;
+                }
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(save);
+                if (st) return st;
+                int err = 0;
+                CKC(step_read_error(ctx->plan, &err, ctx->stream));
+                if (err) return fail(ctx, BEC_ERR_CUDA, "fused step: a dependency wait gave up");
+                how = "autotuned";
+                step_plan_remember(geoms, cand);
+            } else {
+                cudaGetLastError();
+            }
+        }
+    }
+    if (step_plan_build(ctx->plan, geoms, devs, offs, cand, ctx->stream) != cudaSuccess)
+        return fail(ctx, BEC_ERR_CUDA, "fused step plan");
+    CKC(cudaStreamSynchronize(ctx->stream));
+    for (int ci : idx) ctx->fused[ci] = 1;
+    ctx->plan_mode = cand;
+    char buf[512];
+    std::string t = "[";
+    for (int k = 0; k < kStepCandidates; ++k) {
+        std::snprintf(buf, sizeof buf, "%s%.4f", k ? ", " : "", tms[k]);
+        t += buf;
+    }
+    t += "]";
+    std::snprintf(buf, sizeof buf,
+                  "{\"plan\": \"%s\", \"candidate\": %d, \"chosen\": \"%s\", \"grid\": %d, \"items\": %d, "
+                  "\"fused_classes\": %d, \"launches_per_step\": %d, \"candidate_ms_per_step\": ",
+                  step_plan_name(cand), cand, how.c_str(), ctx->plan.grid, ctx->plan.n_items, (int)idx.size(),
+                  ctx->plan.two_phase ? 2 : 1);
+    ctx->plan_desc = std::string(buf) + t + "}";
     return BEC_OK;
 }
 
@@ -437,6 +600,15 @@ bec_status batched_resolve(bec_ctx *ctx, bool observe)
     return BEC_OK;
 }
 
+// Error flag of the fused step kernel: a dependency wait that gave up (the kernel bounds every wait).
+bec_status check_step_error(bec_ctx *ctx)
+{
+    int err = 0;
+    CKC(step_read_error(ctx->plan, &err, ctx->stream));
+    if (err) return fail(ctx, BEC_ERR_CUDA, "fused step: a dependency wait gave up (state of that step is invalid)");
+    return BEC_OK;
+}
+
 // ---------------------------------------------------------------- captured step loop
 // A steady step (the previous step's second half-kick pending, no pulse, no observation) launches the
 // same kernels with the same arguments every time: the full kick in the pencil passes, an increment of
@@ -454,8 +626,7 @@ bec_status capture_steps(bec_ctx *ctx, int k, cudaGraphExec_t *out, long long *k
     }
     bec_status st = BEC_OK;
     for (int i = 0; i < k && st == BEC_OK; ++i) {
-        st = batched_zpass_all(ctx, 0.5f, 0.5f, false, nullptr);
-        if (st == BEC_OK) st = batched_ppass_all(ctx, nullptr, false);
+        st = batched_step(ctx, 0.5f, false);
     }
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     *kernels = g_launches - l0;
@@ -490,15 +661,14 @@ bec_status run_steady(bec_ctx *ctx, long long m)
     }
     if (!graphs) {
         for (long long i = 0; i < m; ++i) {
-            bec_status st = batched_zpass_all(ctx, 0.5f, 0.5f, false, nullptr);
+            bec_status st = batched_step(ctx, 0.5f, true);
             if (st) return st;
-            if ((st = batched_ppass_all(ctx))) return st;
             ctx->step++;
             ctx->evo_steps++;
         }
         return BEC_OK;
     }
-    fp32_put_step(ctx->d_step, (uint32_t)(ctx->step - 1), ctx->stream);   // each replayed step increments first
+    fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);   // each replayed step advances it at its end
     CKL();
     for (long long i = 0; i < m / kGraphSteps; ++i) {
         CKC(cudaGraphLaunch(ctx->step_graph[0], ctx->stream));
@@ -563,10 +733,10 @@ bec_status do_evolve(bec_ctx *ctx, int n)
         }
     } else {
         int s = 0;
+        if ((st = ensure_plan(ctx))) return st;
         if (n > 0 && (!ctx->pending || ctx->has_pulse)) {      // an eager first step starts the stretch
-            if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
+            if ((st = batched_step(ctx, ctx->pending ? 0.5f : 0.0f, true))) return st;
             ctx->pending = true;
-            if ((st = batched_ppass_all(ctx))) return st;
             ctx->step++;
             ctx->evo_steps++;
             s = 1;
@@ -854,6 +1024,7 @@ void bec_destroy(bec_ctx *ctx)
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (void *p : ctx->allocs) cudaFree(p);
+    step_plan_free(ctx->plan);
     for (auto &t : ctx->ws_tables) cudaFree(t.d_basis);
     for (auto &g : ctx->step_graph)
         if (g) cudaGraphExecDestroy(g);
@@ -1632,7 +1803,7 @@ bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps)
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->last_ms = ms;
     ctx->last_launches = g_launches - l0;
-    return BEC_OK;
+    return check_step_error(ctx);
 }
 
 bec_status bec_pulse(bec_ctx *ctx, double theta, double phi)
@@ -1667,7 +1838,7 @@ bec_status bec_pulse_finite(bec_ctx *ctx, double rabi_hz, double duration_s, dou
     }
     ctx->last_launches = g_launches - l0;
     CKC(cudaStreamSynchronize(ctx->stream));
-    return BEC_OK;
+    return check_step_error(ctx);
 }
 
 bec_status bec_start_evolution(bec_ctx *ctx)
@@ -1685,7 +1856,7 @@ bec_status bec_start_evolution(bec_ctx *ctx)
     if ((st = apply_pulse(ctx, m))) return st;
     ctx->evo_steps = 0;
     CKC(cudaStreamSynchronize(ctx->stream));
-    return BEC_OK;
+    return check_step_error(ctx);
 }
 
 bec_status bec_moments_now(bec_ctx *ctx, bec_moments *out)
@@ -1818,6 +1989,7 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
     for (auto &g : ctx->groups) axial_stride += (size_t)4 * g.d.nvz;
     double2 pi_m[4];
     rotation(M_PI, 0.0, pi_m);
+    if ((st = ensure_plan(ctx))) return st;
     const long long l0 = g_launches;
     CKC(cudaEventRecord(ctx->ev0, ctx->stream));
     int sample = 0;
@@ -1875,9 +2047,8 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
                 while (i + len <= n && !event_before(i + len)) ++len;
                 if ((st = run_steady(ctx, len))) return st;
             } else {
-                if ((st = batched_zpass_all(ctx, ctx->pending ? 0.5f : 0.0f, 0.5f, false, nullptr))) return st;
+                if ((st = batched_step(ctx, ctx->pending ? 0.5f : 0.0f, true))) return st;
                 ctx->pending = true;
-                if ((st = batched_ppass_all(ctx))) return st;
                 ctx->step++;
                 ctx->evo_steps++;
             }
@@ -1893,7 +2064,7 @@ bec_status bec_run(bec_ctx *ctx, const bec_schedule *sch, bec_moments *samples, 
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->last_ms = ms;
     ctx->last_launches = g_launches - l0;
-    return BEC_OK;
+    return check_step_error(ctx);
 }
 
 bec_status bec_observables(const bec_ctx *ctx, int32_t group, const bec_moments *m, bec_obs *out)
@@ -2102,6 +2273,59 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
 
 int64_t bec_step_index(const bec_ctx *ctx) { return ctx ? ctx->step : -1; }
 int64_t bec_evolution_steps(const bec_ctx *ctx) { return ctx ? ctx->evo_steps : -1; }
+
+bec_status bec_profile_fused_step(bec_ctx *ctx, int32_t n_steps, double *ms_per_step, int64_t *cells)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (n_steps < 1 || !ms_per_step || !cells) return fail(ctx, BEC_ERR_INVALID_ARG, "bad arguments");
+    if (ctx->path != BEC_PATH_FP32_BATCHED) return fail(ctx, BEC_ERR_STATE, "batched path only");
+    bec_status st = check_ready(ctx);
+    if (st) return st;
+    if ((st = ensure_plan(ctx))) return st;
+    if (!ctx->plan.ready) return fail(ctx, BEC_ERR_STATE, "no fused step plan (no register-path grid class)");
+    if (!ctx->pending || ctx->has_pulse) {
+        if ((st = batched_step(ctx, ctx->pending ? 0.5f : 0.0f, true))) return st;
+        ctx->pending = true;
+        ctx->step++;
+        ctx->evo_steps++;
+    }
+    double tot = 0.0;
+    long long l0 = g_launches;
+    for (int i = 0; i < n_steps; ++i) {
+        fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
+        if ((st = batched_zpass_all(ctx, 0.5f, 0.5f, false, nullptr, false, nullptr, true))) return st;
+        if ((st = batched_ppass_all(ctx, nullptr, false, true))) return st;
+        CKC(cudaEventRecord(ctx->ev0, ctx->stream));
+        step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, 1.0f, nullptr, ctx->stream);
+        CKC(cudaEventRecord(ctx->ev1, ctx->stream));
+        CKC(cudaEventSynchronize(ctx->ev1));
+        CKL();
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        tot += ms;
+        ctx->step++;
+        ctx->evo_steps++;
+    }
+    ctx->last_launches = g_launches - l0;
+    long long n = 0;
+    for (size_t ci = 0; ci < ctx->classes.size(); ++ci)
+        if (ctx->fused[ci]) n += (long long)ctx->classes[ci].geom.n_traj * ctx->classes[ci].geom.cells;
+    *ms_per_step = tot / n_steps;
+    *cells = n;
+    return check_step_error(ctx);
+}
+
+bec_status bec_step_plan(bec_ctx *ctx, char *out, int32_t len)
+{
+    if (!ctx) return BEC_ERR_INVALID_ARG;
+    if (!out || len < 1) return fail(ctx, BEC_ERR_INVALID_ARG, "null output");
+    const std::string d = ctx->path != BEC_PATH_FP32_BATCHED ? std::string("{\"plan\": \"plain path\"}")
+                          : ctx->plan_mode == -2 ? std::string("{\"plan\": \"not chosen (no step taken)\"}")
+                                                 : ctx->plan_desc;
+    if ((int32_t)d.size() >= len) return fail(ctx, BEC_ERR_INVALID_ARG, "output buffer too small");
+    std::memcpy(out, d.c_str(), d.size() + 1);
+    return BEC_OK;
+}
 
 int32_t bec_step_graphs(const bec_ctx *ctx)
 {

@@ -184,6 +184,20 @@ __host__ __device__ __forceinline__ int brev_bits(int v, int bits)
 template <typename R>
 __host__ __device__ __forceinline__ R getk(int i, R dk, int n) { return (2 * i > n) ? dk * (R)(i - n) : dk * (R)i; }
 
+// signed index of lattice index i along an axis of n points (k = dk * kidx(i, n), getK)
+__host__ __device__ __forceinline__ int kidx(int i, int n) { return (2 * i > n) ? i - n : i; }
+
+// e^{+2 pi i turns}, turns = frac (c_x ix^2 + c_y iy^2 + c_z iz^2) formed in FP64 (GroupParamsF::kin_*):
+// the kinetic phase e^{+i k^2/2 dt frac} (wigner_kernel.cu:137-151) reduced to [-1/2, 1/2] turn
+// exactly and rounded once, to FP32
+__device__ __forceinline__ float2 kin_phase(double turns)
+{
+    const double r = turns - rint(turns);
+    double s, c;
+    sincospi(2.0 * r, &s, &c);
+    return make_float2((float)c, (float)s);
+}
+
 // Neumaier-compensated accumulator.
 struct KSum {
     double s, c;

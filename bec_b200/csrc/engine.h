@@ -33,6 +33,10 @@ struct GroupParamsF {
     float init_a, init_b;     // Va / sqrt(dV), Vb / sqrt(dV)
     int itmax, noise;
     uint32_t seed_lo, seed_hi;
+    // kinetic phase per unit index squared in turns, 0.5 dk^2 dt_evo / (2 pi) per axis (ky term 0 in
+    // 2D): the angle 0.5 k^2 dt reaches several radians at the largest k, so it is formed in FP64 from
+    // exact integer indices, k = dk * i, and only its sine and cosine are rounded to FP32
+    double kin_x, kin_y, kin_z;
 };
 
 // Geometry of one grid class of the batched path (all trajectories sharing nx, ny, nz).
@@ -187,3 +191,54 @@ void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp,
                       const float2 *tw_full, float frac, float scale, const float2 *m, double *obs,
                       float out_scale, cudaStream_t s);
 int fp32_fast_pencil_tiles(const ClassGeom &c);
+
+// step_kernel.cu: one launch per split step for the classes of the register passes. Items of the work
+// list are int4 (kind | class << 4, class-local trajectory, item index within the trajectory, counter
+// index of the trajectory).
+struct StepClassDev {
+    float4 *state;
+    const int *tgroup, *tlocal;
+    const float2 *tw;         // W_nz^e, e < nz
+    int nx, ny, nz, lx, cells, tiles, n_traj;
+    int pencil_items;         // pencil items per trajectory (filled by step_plan_build)
+};
+struct StepLaunch {
+    const StepClassDev *cls;
+    const GroupParamsF *gp;
+    const int4 *items;
+    int n_items;
+    int *queue, *finished, *err, *done;
+    int n_counters;
+    uint32_t *d_step;
+    int wait, inc_step;
+    int stall;                // added to every plane item's dependency count (fault injection in tests)
+    unsigned long long wait_limit_ns;
+};
+constexpr int kStepCandidates = 5;     // two-phase, then interleaved at 0.5, 1, 2, 4 waves
+struct StepPlan {
+    bool ready = false;
+    int candidate = -1;
+    bool two_phase = false;
+    int grid = 0, n_items = 0, n_pencil = 0, n_plane = 0, n_counters = 0;
+    int4 *d_items = nullptr;
+    StepClassDev *d_cls = nullptr;
+    int *d_counters = nullptr;          // queue, finished, error flag, pad, then one per trajectory
+    int stall = 0;                      // BEC_STEP_INJECT_STALL: plane items wait for a count never reached
+    unsigned long long wait_limit_ns = 2000000000ull;   // BEC_STEP_WAIT_LIMIT_MS
+};
+bool step_class_supported(const ClassGeom &c);
+const char *step_plan_name(int candidate);
+// builds (or rebuilds, reusing the buffers) the work list of candidate `candidate` for the classes geoms
+// (cls: their device descriptors; traj_offset: first counter index of each)
+cudaError_t step_plan_build(StepPlan &P, const std::vector<ClassGeom> &geoms, const std::vector<StepClassDev> &cls,
+                            const std::vector<int> &traj_offset, int candidate, cudaStream_t s);
+void step_plan_free(StepPlan &P);
+// one split step (kick fraction frac of dt, optional pulse matrix m) of every class in the plan; the
+// last CTA advances *d_step
+void step_launch(const StepPlan &P, const GroupParamsF *gp, uint32_t *d_step, float frac, const float2 *m,
+                 cudaStream_t s);
+// *err = 1 if a dependency wait of a launch since the plan was built gave up (synchronises s)
+cudaError_t step_read_error(const StepPlan &P, int *err, cudaStream_t s);
+// per-process cache of the autotuned candidate for a class mix on this device (-1: none)
+int step_plan_cached(const std::vector<ClassGeom> &geoms);
+void step_plan_remember(const std::vector<ClassGeom> &geoms, int candidate);

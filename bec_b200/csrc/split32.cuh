@@ -86,29 +86,30 @@ __device__ __forceinline__ void dif_recv(T *v, const T *xi, std::integer_sequenc
 
 using Seq8 = std::make_integer_sequence<int, 8>;
 
-// forward: v[j] = x[2j + h] -> v[s] = X[kblk(s, h)]; xb: the plane's exchange slots [2][8][32]
-template <typename T>
-__device__ __forceinline__ void fwd_line(T *v, T *xb, int h, int lane)
+// forward: v[j] = x[2j + h] -> v[s] = X[kblk(s, h)]; xb: the plane's exchange slots [2][8][32];
+// bar(): the barrier of the plane's two warps
+template <typename T, typename Bar>
+__device__ __forceinline__ void fwd_line(T *v, T *xb, int h, int lane, Bar bar)
 {
     fftreg::dft<16, false>(v);
     T *xo = xb + h * 256 + lane;
     const T *xi = xb + (1 - h) * 256 + lane;
     if (h == 0) dit_send<0>(v, xo, Seq8{});
     else dit_send<1>(v, xo, Seq8{});
-    __syncthreads();
+    bar();
     if (h == 0) dit_recv<0>(v, xi, Seq8{});
     else dit_recv<1>(v, xi, Seq8{});
 }
 
 // inverse (unnormalised): v[s] = x[kblk(s, h)] -> v[m] = y[2m + h]
-template <typename T>
-__device__ __forceinline__ void inv_line(T *v, T *xb, int h, int lane)
+template <typename T, typename Bar>
+__device__ __forceinline__ void inv_line(T *v, T *xb, int h, int lane, Bar bar)
 {
     T *xo = xb + h * 256 + lane;
     const T *xi = xb + (1 - h) * 256 + lane;
     if (h == 0) dif_send<0>(v, xo, Seq8{});
     else dif_send<1>(v, xo, Seq8{});
-    __syncthreads();
+    bar();
     if (h == 0) dif_recv<0>(v, xi, Seq8{});
     else dif_recv<1>(v, xi, Seq8{});
     fftreg::dft<16, true>(v);

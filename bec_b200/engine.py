@@ -55,6 +55,8 @@ SIGNATURES = {
     "bec_checkpoint_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "bec_checkpoint_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "bec_step_graphs": (C.c_int32, [C.c_void_p]),
+    "bec_step_plan": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "bec_profile_fused_step": (C.c_int, [C.c_void_p, C.c_int32, _dp, _P(C.c_int64)]),
     "bec_last_device_ms": (C.c_double, [C.c_void_p]),
     "bec_last_launch_count": (C.c_int64, [C.c_void_p]),
     "bec_profile_steps": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P(C.c_int32), _P(C.c_int64), _dp,
@@ -186,6 +188,14 @@ class Engine:
         """Loads a checkpoint of a context with the same groups and path (bec_checkpoint_load)."""
         buf = C.create_string_buffer(bytes(blob), len(blob))
         self._check(lib().bec_checkpoint_load(self._h, buf, len(blob)), "bec_checkpoint_load")
+
+    @property
+    def step_plan(self):
+        """The split-step schedule (bec_step_plan) as a dict."""
+        import json
+        buf = C.create_string_buffer(4096)
+        self._check(lib().bec_step_plan(self._h, buf, len(buf)), "bec_step_plan")
+        return json.loads(buf.value.decode())
 
     @property
     def step_graphs(self):
@@ -368,6 +378,14 @@ class Engine:
             raise ValueError("basis shape")
         self._check(lib().bec_warmstart_set_basis(self._h, nx, ny, nz, b.shape[0], b.ctypes.data_as(_P(C.c_float))),
                     "bec_warmstart_set_basis")
+
+    def profile_fused_step(self, n_steps):
+        """(mean ms of one step's fused launch, cells it covers) over n_steps steady steps."""
+        ms = C.c_double()
+        cells = C.c_int64()
+        self._check(lib().bec_profile_fused_step(self._h, int(n_steps), C.byref(ms), C.byref(cells)),
+                    "bec_profile_fused_step")
+        return ms.value, int(cells.value)
 
     def profile_steps(self, n_steps, max_classes=16):
         """Per grid class: dict(dims, traj, z_ms, plane_ms) mean device time per launch."""

@@ -25,22 +25,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# ncu: DRAM bytes (read + write) of one launch divided by its trajectory count,
-# from captures of a 64-trajectory 32x32x256 class; traffic scales with the
-# trajectories a launch processes. Algorithmic: 32 B x 262144 cells = 8.39 MB
-# per trajectory.
-NCU_TRAFFIC_PER_TRAJ = {
-    "plane_32x32x256": (268.500224e6 + 210.539776e6) / 64,
-    "pencil_32x32x256": (268.492800e6 + 209.569280e6) / 64,
-}
+# ncu: DRAM bytes (read + write) per cell of one launch of the fused step kernel, from a capture of a
+# smaller uneven batch; traffic scales with the cells a launch processes (algorithmic: 32 B per cell).
+NCU_TRAFFIC_PER_CELL = {}
 
 # ncu: thread-instructions per cell of one launch (smsp__inst_executed.sum x 32 / cells), from the same
-# captures. With the launch time they give the kernel's instruction issue rate, whose ceiling is one
+# capture. With the launch time they give the kernel's instruction issue rate, whose ceiling is one
 # warp-instruction per scheduler per clock: SMs x 4 x 32 thread-instructions per clock.
-NCU_INSTR_PER_CELL = {
-    "plane_32x32x256": 193569962 * 32 / (64 * 262144),
-    "pencil_32x32x256": 68464640 * 32 / (64 * 262144),
-}
+NCU_INSTR_PER_CELL = {}
 
 N_TRAJ = 1024
 WORKLOAD = "uneven-ensembles-1024"
@@ -283,23 +275,28 @@ def main():
     n_traj_total = args.n_traj * ws
     value = n_traj_total * args.steps / (ms * 1e-3)
 
-    # per-kernel device times of the same workload (CUDA events on the engine's stream)
-    prof = eng.profile_steps(3)
+    # device time of the dominant kernel: the fused step kernel (one launch per step covering every grid
+    # class, CUDA events on the engine's stream), and the per-pass kernels of the launch-per-pass schedule
+    plan = eng.step_plan
     peak, peak_kind = peaks()
+    fused_ms, fused_cells = eng.profile_fused_step(5)
+    prof = eng.profile_steps(3)
     kernels = []
     for c in prof:
         nx, ny, nz = c["dims"]
         bytes_launch = 32.0 * nx * ny * nz * c["traj"]      # read + write of both complex64 components
         for kind, t in (("pencil", c["z_ms"]), ("plane", c["plane_ms"])):
             kernels.append(dict(kernel=f"{kind}_{nx}x{ny}x{nz}", ms=t, bytes=bytes_launch, traj=c["traj"]))
-    dom = max(kernels, key=lambda k: k["ms"])
+    dom = dict(kernel="k_step", ms=fused_ms, bytes=32.0 * fused_cells, cells=fused_cells)
     achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
-    traffic = None
-    if NCU_TRAFFIC_PER_TRAJ and dom["kernel"] in NCU_TRAFFIC_PER_TRAJ:
-        traffic = NCU_TRAFFIC_PER_TRAJ[dom["kernel"]] * dom["traj"]
-    roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                "algorithmic_bytes": dom["bytes"], "ms_per_launch": dom["ms"]}
+    traffic = NCU_TRAFFIC_PER_CELL["k_step"] * fused_cells if "k_step" in NCU_TRAFFIC_PER_CELL else None
+    roofline = {"bound": "hbm", "kernel": "k_step (fused split step, every grid class, one launch)",
+                "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": dom["bytes"],
+                "ms_per_launch": dom["ms"],
+                "note": "32 B per cell and step (both complex64 components read and written once); the kernel "
+                        "does both passes of the step"}
+    per_pass = {k["kernel"]: {"ms": k["ms"], "frac": k["bytes"] / (k["ms"] * 1e-3) / 1e9 / peak} for k in kernels}
     step_gbs = 32.0 * total_cells * args.steps / (ms * 1e-3) / 1e9 * (ws if ws > 1 else 1)
     step_roof = {"achieved": step_gbs / ws if ws > 1 else step_gbs, "peak": peak, "unit": "GB/s",
                  "frac": (step_gbs / ws if ws > 1 else step_gbs) / peak,
@@ -371,8 +368,7 @@ def main():
     clocks = clk.summary()
     issue_roof = None
     if dom["kernel"] in NCU_INSTR_PER_CELL:
-        nx, ny, nz = (int(v) for v in dom["kernel"].split("_")[1].split("x"))
-        instr = NCU_INSTR_PER_CELL[dom["kernel"]] * nx * ny * nz * dom["traj"]
+        instr = NCU_INSTR_PER_CELL[dom["kernel"]] * dom["cells"]
         mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         if mhz:
@@ -394,7 +390,8 @@ def main():
                        "trap_jitter": "+-10%", "dt_s": 4e-5, "noise": "Philox vacuum + loss noise",
                        "l2": f"state {16 * total_cells / 1e9:.2f} GB per GPU, larger than L2",
                        "parallelism": f"dp{ws} (trajectory sharding)", "path": "fp32-batched"},
-            "roofline": roofline, "issue_roofline": issue_roof, "step_roofline": step_roof, "cpu_baseline": cpu,
+            "roofline": roofline, "issue_roofline": issue_roof, "step_roofline": step_roof,
+            "step_plan": plan, "per_pass_kernels": per_pass, "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, **extras,
         }

@@ -9,6 +9,7 @@ from bec_b200.engine import Engine
 from oracle import oracle as O
 
 LOG = os.environ.get("BEC_PARITY_LOG")
+DUMP = os.environ.get("BEC_PARITY_DUMP")
 
 
 def record(name, **vals):
@@ -17,6 +18,14 @@ def record(name, **vals):
         return
     with open(LOG, "a") as f:
         f.write(json.dumps({"test": name, **{k: float(v) for k, v in vals.items()}}) + "\n")
+
+
+def dump(name, **arrays):
+    """Saves arrays to $BEC_PARITY_DUMP/<name>.npz when set (for offline error analysis)."""
+    if not DUMP:
+        return
+    os.makedirs(DUMP, exist_ok=True)
+    np.savez_compressed(os.path.join(DUMP, name + ".npz"), **arrays)
 
 
 def rel_state_err(a, b):

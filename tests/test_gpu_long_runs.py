@@ -23,7 +23,7 @@ from bec_b200 import observables as OBS
 from bec_b200._abi import BEC_GS_FIXED_STEPS
 from bec_b200.configs import copy_params, ensemble_16x16x128, spin_echo_32x32x256
 from bec_b200.engine import BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, Engine
-from parity_util import record
+from parity_util import dump, record
 
 pytestmark = pytest.mark.gpu
 
@@ -94,6 +94,7 @@ def _compare(name, p, meta, fx, eng, mom, traj, axial):
         worst_ratio = max(worst_ratio, float(np.abs(OBS.axial_ratio(ae, d, p.ne) - OBS.axial_ratio(ao, d, p.ne))[keep].max()))
     err["axial_ratio"] = worst_ratio
     record(name, **err)
+    dump(name, moments=mom, traj_moments=traj, axial=axial)
     return err
 
 
