@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "twiddle_fp32.h"
 
 namespace {
 
@@ -60,6 +61,7 @@ struct ClassRec {
     int obs_tiles = 1;        // tiles of the pass that last wrote obs_partial
     int traj_offset = 0;      // global index of the class's first trajectory
     std::vector<int> groups;  // group indices in this class
+    float2 *kin_tab[2] = {nullptr, nullptr};   // kinetic phase tables for kick fractions 0.5 and 1 (register pencils)
 };
 
 } // namespace
@@ -72,6 +74,7 @@ struct bec_ctx {
     std::map<int, double2 *> tw64;
     std::map<int, float2 *> tw32;
     std::map<int, float2 *> tw32_full;
+    std::map<int, float2 *> tw32_nearest;
     bool use_fast = true;                // register-resident passes where the shape allows
     uint32_t *d_step = nullptr;          // batched: Philox step index the plane passes read
     bool use_graphs = true;              // batched: steady steps replay captured CUDA graphs
@@ -249,13 +252,27 @@ bec_status get_tw64(bec_ctx *ctx, int n, double2 **out)
     return BEC_OK;
 }
 
+// W_n^k = e^{-2 pi i k / n} in FP32: exact at multiples of a quarter turn, elsewhere the pair of modulus
+// closest to 1 (twiddle_fp32.h)
+float2 tw32_unit(int k, int n)
+{
+    k %= n;
+    if ((4 * k) % n == 0) {
+        const int q = 4 * k / n;
+        return q == 0 ? make_float2(1.f, 0.f) : q == 1 ? make_float2(0.f, -1.f) : q == 2 ? make_float2(-1.f, 0.f)
+                                                                                    : make_float2(0.f, 1.f);
+    }
+    const double a = 2.0 * M_PI * (double)k / (double)n;
+    const fftreg::Twid t = fftreg::unit_cs(std::cos(a), -std::sin(a));
+    return make_float2(t.a, t.b);
+}
+
 bec_status get_tw32(bec_ctx *ctx, int n, float2 **out)
 {
     auto it = ctx->tw32.find(n);
     if (it != ctx->tw32.end()) { *out = it->second; return BEC_OK; }
-    std::vector<double2> t = twiddles(n);
-    std::vector<float2> f(t.size());
-    for (size_t i = 0; i < t.size(); ++i) f[i] = make_float2((float)t[i].x, (float)t[i].y);
+    std::vector<float2> f(n / 2 > 0 ? n / 2 : 1, make_float2(1.f, 0.f));
+    for (int k = 0; k < n / 2; ++k) f[k] = tw32_unit(k, n);
     float2 *d = nullptr;
     CKC(dalloc(ctx, &d, f.size()));
     CKC(cudaMemcpyAsync(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
@@ -270,14 +287,29 @@ bec_status get_tw32_full(bec_ctx *ctx, int n, float2 **out)
     auto it = ctx->tw32_full.find(n);
     if (it != ctx->tw32_full.end()) { *out = it->second; return BEC_OK; }
     std::vector<float2> f(n);
+    for (int k = 0; k < n; ++k) f[k] = tw32_unit(k, n);
+    float2 *d = nullptr;
+    CKC(dalloc(ctx, &d, f.size()));
+    CKC(cudaMemcpyAsync(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->tw32_full[n] = d;
+    *out = d;
+    return BEC_OK;
+}
+
+// W_n^e, e < n, rounded to the nearest FP32 values (the imaginary-time passes; see tw32_unit)
+bec_status get_tw32_full_nearest(bec_ctx *ctx, int n, float2 **out)
+{
+    auto it = ctx->tw32_nearest.find(n);
+    if (it != ctx->tw32_nearest.end()) { *out = it->second; return BEC_OK; }
+    std::vector<float2> f(n);
     for (int k = 0; k < n; ++k) {
-        double a = 2.0 * M_PI * (double)k / (double)n;
+        const double a = 2.0 * M_PI * (double)k / (double)n;
         f[k] = make_float2((float)std::cos(a), (float)-std::sin(a));
     }
     float2 *d = nullptr;
     CKC(dalloc(ctx, &d, f.size()));
     CKC(cudaMemcpyAsync(d, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
-    ctx->tw32_full[n] = d;
+    ctx->tw32_nearest[n] = d;
     *out = d;
     return BEC_OK;
 }
@@ -351,14 +383,19 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
         z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
         const size_t ci = &c - &ctx->classes[0];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
-        // the register pencil pass observes only when it also ends the step (post = 0)
+        // the register pencil pass observes only when it also ends the step (post = 0), and kicks by the
+        // fractions its kinetic tables hold (0.5, 1) or not at all
+        const float kf = pre + post;
         const bool fast = ctx->use_fast && fp32_fast_pencil_supported(c.geom) &&
+                          (kf == 0.0f || kf == 0.5f || kf == 1.0f) &&
                           (!observe || (post == 0.0f && ends_step && !z.has_m2));
         if (fast) {
             float2 *twf;
             if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
-            fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, pre + post, z.scale * z.out_scale,
-                             mf, observe ? c.obs_partial : nullptr, z.out_scale, ctx->stream);
+            const float frac = kf;
+            const float2 *kin = frac == 1.0f ? c.kin_tab[1] : frac == 0.5f ? c.kin_tab[0] : nullptr;
+            fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, frac, z.scale * z.out_scale,
+                             mf, observe ? c.obs_partial : nullptr, z.out_scale, kin, ctx->stream);
             if (observe) c.obs_tiles = fp32_fast_pencil_tiles(c.geom);
         } else {
             float2 *tz;
@@ -453,6 +490,8 @@ bec_status ensure_plan(bec_ctx *ctx)
             d.tw = twf;
             d.nx = c.geom.nx; d.ny = c.geom.ny; d.nz = c.geom.nz; d.lx = c.geom.lx;
             d.cells = c.geom.cells; d.tiles = c.geom.nx * c.geom.ny / 16; d.n_traj = c.geom.n_traj;
+            d.kin[0] = c.kin_tab[0];
+            d.kin[1] = c.kin_tab[1];
             geoms.push_back(c.geom);
             devs.push_back(d);
             offs.push_back(c.traj_offset);
@@ -464,44 +503,48 @@ bec_status ensure_plan(bec_ctx *ctx)
         ctx->plan_desc = "{\"plan\": \"unfused\", \"launches_per_step\": \"2 per class\"}";
         return BEC_OK;
     }
-    int cand = -1;
-    std::string how;
-    std::vector<double> tms(kStepCandidates, -1.0);
+    // candidates: -1 = two launches per class (per-pass kernels), 0 .. kStepCandidates-1 = fused work lists
+    int cand = 2;
+    std::string how = "default";
+    std::vector<double> tms(kStepCandidates + 1, -1.0);   // [0]: per-pass launches, [k + 1]: candidate k
     if (force && *force) {
         cand = std::atoi(force);
         if (cand < 0 || cand >= kStepCandidates) return fail(ctx, BEC_ERR_INVALID_ARG, "BEC_STEP_PLAN out of range");
         how = "forced";
-    } else if ((cand = step_plan_cached(geoms)) >= 0) {
+    } else if (step_plan_cached(geoms, &cand)) {
         how = "cached";
     } else {
         const char *at = std::getenv("BEC_AUTOTUNE");
-        cand = 2;
-        how = "default";
         if (!(at && at[0] == '0')) {
-            // time every candidate on a copy of the state: the copy is restored afterwards, so tuning
-            // changes nothing of the run (every candidate computes the same bits anyway)
+            // time every candidate's full step on a copy of the state: the copy (and any pending pulse) is
+            // restored afterwards, so tuning changes nothing of the run; every candidate computes the same bits
             size_t bytes = 0;
-            for (const ClassGeom &g : geoms) bytes += sizeof(float4) * (size_t)g.n_traj * g.cells;
+            for (auto &c : ctx->classes) bytes += sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
             char *save = nullptr;
             if (cudaMalloc(&save, bytes) == cudaSuccess) {
                 size_t o = 0;
-                for (const StepClassDev &d : devs) {
-                    const size_t n = sizeof(float4) * (size_t)d.n_traj * d.cells;
-                    CKC(cudaMemcpyAsync(save + o, d.state, n, cudaMemcpyDeviceToDevice, ctx->stream));
+                for (auto &c : ctx->classes) {
+                    const size_t n = sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
+                    if (n) CKC(cudaMemcpyAsync(save + o, c.state, n, cudaMemcpyDeviceToDevice, ctx->stream));
                     o += n;
                 }
+                const bool had_pulse = ctx->has_pulse;
+                ctx->has_pulse = false;
                 bec_status st = BEC_OK;
                 double best = 1e30;
-                for (int k = 0; k < kStepCandidates && st == BEC_OK; ++k) {
-                    if (step_plan_build(ctx->plan, geoms, devs, offs, k, ctx->stream) != cudaSuccess) {
+                for (int k = -1; k < kStepCandidates && st == BEC_OK; ++k) {
+                    if (k < 0) {
+                        ctx->plan.ready = false;
+                    } else if (step_plan_build(ctx->plan, geoms, devs, offs, k, ctx->stream) != cudaSuccess) {
                         st = fail(ctx, BEC_ERR_CUDA, "fused step plan");
                         break;
                     }
-                    fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
-                    step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, 1.0f, nullptr, ctx->stream);
-                    cudaEventRecord(ctx->ev0, ctx->stream);
-                    for (int r = 0; r < 3; ++r)
-                        step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, 1.0f, nullptr, ctx->stream);
+                    for (int ci : idx) ctx->fused[ci] = k >= 0;
+                    for (int r = 0; r < 4 && st == BEC_OK; ++r) {
+                        if (r == 1) cudaEventRecord(ctx->ev0, ctx->stream);
+                        st = batched_step(ctx, 0.5f, true);
+                    }
+                    if (st) break;
                     cudaEventRecord(ctx->ev1, ctx->stream);
                     if (cudaEventSynchronize(ctx->ev1) != cudaSuccess) {
                         st = fail(ctx, BEC_ERR_CUDA, std::string("fused step: ") + cudaGetErrorString(cudaGetLastError()));
@@ -509,17 +552,19 @@ bec_status ensure_plan(bec_ctx *ctx)
                     }
                     float ms = 0.f;
                     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-                    tms[k] = ms / 3.0;
-                    if (tms[k] < best) { best = tms[k]; cand = k; }
+                    tms[k + 1] = ms / 3.0;
+                    if (tms[k + 1] < best) { best = tms[k + 1]; cand = k; }
                 }
                 o = 0;
-                for (const StepClassDev &d : devs) {
-                    const size_t n = sizeof(float4) * (size_t)d.n_traj * d.cells;
-                    cudaMemcpyAsync(d.state, save + o, n, cudaMemcpyDeviceToDevice, ctx->stream);
+                for (auto &c : ctx->classes) {
+                    const size_t n = sizeof(float4) * (size_t)c.geom.n_traj * c.geom.cells;
+                    if (n) cudaMemcpyAsync(c.state, save + o, n, cudaMemcpyDeviceToDevice, ctx->stream);
                     o += n;
                 }
                 cudaStreamSynchronize(ctx->stream);
                 cudaFree(save);
+                ctx->has_pulse = had_pulse;
+                std::fill(ctx->fused.begin(), ctx->fused.end(), 0);
                 if (st) return st;
                 int err = 0;
                 CKC(step_read_error(ctx->plan, &err, ctx->stream));
@@ -531,24 +576,34 @@ bec_status ensure_plan(bec_ctx *ctx)
             }
         }
     }
+    char buf[512];
+    std::string t = "[";
+    for (int k = 0; k <= kStepCandidates; ++k) {
+        std::snprintf(buf, sizeof buf, "%s%.4f", k ? ", " : "", tms[k]);
+        t += buf;
+    }
+    t += "]";
+    if (cand < 0) {
+        ctx->plan.ready = false;
+        ctx->plan_mode = -1;
+        std::snprintf(buf, sizeof buf,
+                      "{\"plan\": \"%s\", \"candidate\": -1, \"chosen\": \"%s\", \"fused_classes\": 0, "
+                      "\"launches_per_step\": %d, \"candidate_ms_per_step\": ",
+                      step_plan_name(-1), how.c_str(), 2 * (int)idx.size());
+        ctx->plan_desc = std::string(buf) + t + ", \"candidates\": \"per-pass launches, then fused 0..4\"}";
+        return BEC_OK;
+    }
     if (step_plan_build(ctx->plan, geoms, devs, offs, cand, ctx->stream) != cudaSuccess)
         return fail(ctx, BEC_ERR_CUDA, "fused step plan");
     CKC(cudaStreamSynchronize(ctx->stream));
     for (int ci : idx) ctx->fused[ci] = 1;
     ctx->plan_mode = cand;
-    char buf[512];
-    std::string t = "[";
-    for (int k = 0; k < kStepCandidates; ++k) {
-        std::snprintf(buf, sizeof buf, "%s%.4f", k ? ", " : "", tms[k]);
-        t += buf;
-    }
-    t += "]";
     std::snprintf(buf, sizeof buf,
                   "{\"plan\": \"%s\", \"candidate\": %d, \"chosen\": \"%s\", \"grid\": %d, \"items\": %d, "
                   "\"fused_classes\": %d, \"launches_per_step\": %d, \"candidate_ms_per_step\": ",
                   step_plan_name(cand), cand, how.c_str(), ctx->plan.grid, ctx->plan.n_items, (int)idx.size(),
                   ctx->plan.two_phase ? 2 : 1);
-    ctx->plan_desc = std::string(buf) + t + "}";
+    ctx->plan_desc = std::string(buf) + t + ", \"candidates\": \"per-pass launches, then fused 0..4\"}";
     return BEC_OK;
 }
 
@@ -1010,6 +1065,13 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
             CKA(cudaMemcpyAsync(c.d_tgroup, tg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, ctx->stream));
             CKA(cudaMemcpyAsync(c.d_tlocal, tl.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, ctx->stream));
             CKA(cudaMemcpyAsync(c.d_traj_scale, ts.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, ctx->stream));
+            if (fp32_fast_pencil_supported(c.geom)) {
+                for (int k = 0; k < 2; ++k) {
+                    CKA(dalloc(ctx, &c.kin_tab[k], nt * (size_t)(c.geom.nz + c.geom.nx * c.geom.ny)));
+                    fp32_kin_tables(c.kin_tab[k], c.geom, ctx->d_gparams, c.d_tgroup, k ? 1.0f : 0.5f, ctx->stream);
+                }
+                if (cudaGetLastError() != cudaSuccess) return bail(BEC_ERR_CUDA);
+            }
         }
         CKA(dalloc(ctx, &ctx->scratch4, (size_t)ctx->max_cells));
     }
@@ -1344,7 +1406,7 @@ bec_status gs_batched(bec_ctx *ctx, int n, const int32_t *groups, const bec_gs_o
                                 c.warm, s));
         }
     }
-    auto tw_for = [&](int nz, float2 **tw) { return get_tw32_full(ctx, nz, tw); };
+    auto tw_for = [&](int nz, float2 **tw) { return get_tw32_full_nearest(ctx, nz, tw); };
     bec_status st;
     // start: x-space profile -> stored form; measure its norm, first half kick of step 0
     for (auto &c : cls) {

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "twiddle_fp32.h"
+
 #define BEC_HD __host__ __device__ __forceinline__
 
 // ---------------------------------------------------------------- complex
@@ -86,6 +88,37 @@ __device__ __forceinline__ u32x4x2 philox4x32_10_x2(uint32_t a0, uint32_t a1, ui
         k1 += 0xBB67AE85u;
     }
     return u32x4x2{u32x4{a0, a1, a2, a3}, u32x4{b0, b1, b2, b3}};
+}
+
+// Four draws under one key, their rounds interleaved (four independent multiply chains, one key schedule).
+struct u32x4x4 { u32x4 a, b, c, d; };
+
+__device__ __forceinline__ u32x4x4 philox4x32_10_x4(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                    uint32_t k0, uint32_t k1)
+{
+    // counters (c0 + i, c1, c2, c3), i < 4
+    uint32_t a0 = c0, a1 = c1, a2 = c2, a3 = c3;
+    uint32_t b0 = c0 + 1u, b1 = c1, b2 = c2, b3 = c3;
+    uint32_t e0 = c0 + 2u, e1 = c1, e2 = c2, e3 = c3;
+    uint32_t d0 = c0 + 3u, d1 = c1, d2 = c2, d3 = c3;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t la0 = 0xD2511F53u * a0, ha0 = __umulhi(0xD2511F53u, a0);
+        const uint32_t la1 = 0xCD9E8D57u * a2, ha1 = __umulhi(0xCD9E8D57u, a2);
+        const uint32_t lb0 = 0xD2511F53u * b0, hb0 = __umulhi(0xD2511F53u, b0);
+        const uint32_t lb1 = 0xCD9E8D57u * b2, hb1 = __umulhi(0xCD9E8D57u, b2);
+        const uint32_t le0 = 0xD2511F53u * e0, he0 = __umulhi(0xD2511F53u, e0);
+        const uint32_t le1 = 0xCD9E8D57u * e2, he1 = __umulhi(0xCD9E8D57u, e2);
+        const uint32_t ld0 = 0xD2511F53u * d0, hd0 = __umulhi(0xD2511F53u, d0);
+        const uint32_t ld1 = 0xCD9E8D57u * d2, hd1 = __umulhi(0xCD9E8D57u, d2);
+        a0 = ha1 ^ a1 ^ k0; a2 = ha0 ^ a3 ^ k1; a1 = la1; a3 = la0;
+        b0 = hb1 ^ b1 ^ k0; b2 = hb0 ^ b3 ^ k1; b1 = lb1; b3 = lb0;
+        e0 = he1 ^ e1 ^ k0; e2 = he0 ^ e3 ^ k1; e1 = le1; e3 = le0;
+        d0 = hd1 ^ d1 ^ k0; d2 = hd0 ^ d3 ^ k1; d1 = ld1; d3 = ld0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return u32x4x4{u32x4{a0, a1, a2, a3}, u32x4{b0, b1, b2, b3}, u32x4{e0, e1, e2, e3}, u32x4{d0, d1, d2, d3}};
 }
 
 // Stream tags of the counter's fourth word.
@@ -189,13 +222,14 @@ __host__ __device__ __forceinline__ int kidx(int i, int n) { return (2 * i > n) 
 
 // e^{+2 pi i turns}, turns = frac (c_x ix^2 + c_y iy^2 + c_z iz^2) formed in FP64 (GroupParamsF::kin_*):
 // the kinetic phase e^{+i k^2/2 dt frac} (wigner_kernel.cu:137-151) reduced to [-1/2, 1/2] turn
-// exactly and rounded once, to FP32
+// exactly, evaluated in FP64 and rounded to the FP32 pair of modulus closest to 1 (twiddle_fp32.h)
 __device__ __forceinline__ float2 kin_phase(double turns)
 {
     const double r = turns - rint(turns);
     double s, c;
     sincospi(2.0 * r, &s, &c);
-    return make_float2((float)c, (float)s);
+    const fftreg::Twid t = fftreg::unit_cs(c, s);
+    return make_float2(t.a, t.b);
 }
 
 // Neumaier-compensated accumulator.

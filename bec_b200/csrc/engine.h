@@ -187,9 +187,14 @@ void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, 
 // tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times out_scale;
 // m: optional pulse matrix (row-major, 4 entries) or NULL; obs: when not NULL the pass
 // ends a step and writes per-z partial moments [traj][tile][z][4] (tiles = fp32_fast_pencil_tiles)
+// kin: the class's kinetic phase table for frac (fp32_kin_tables), or NULL to evaluate the phases in place
 void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
                       const float2 *tw_full, float frac, float scale, const float2 *m, double *obs,
-                      float out_scale, cudaStream_t s);
+                      float out_scale, const float2 *kin, cudaStream_t s);
+// kinetic phase factors of a class for kick fraction frac: per class-local trajectory t, tab[t * (nz + nx ny) + i]
+// = e^{+i kz_i^2/2 dt frac} for i < nz, then e^{+i (kx^2 + ky^2)/2 dt frac} per pencil (y * nx + x)
+void fp32_kin_tables(float2 *tab, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, float frac,
+                     cudaStream_t s);
 int fp32_fast_pencil_tiles(const ClassGeom &c);
 
 // step_kernel.cu: one launch per split step for the classes of the register passes. Items of the work
@@ -199,6 +204,7 @@ struct StepClassDev {
     float4 *state;
     const int *tgroup, *tlocal;
     const float2 *tw;         // W_nz^e, e < nz
+    const float2 *kin[2];     // kinetic phase tables for kick fractions 0.5 and 1 (fp32_kin_tables)
     int nx, ny, nz, lx, cells, tiles, n_traj;
     int pencil_items;         // pencil items per trajectory (filled by step_plan_build)
 };
@@ -239,6 +245,6 @@ void step_launch(const StepPlan &P, const GroupParamsF *gp, uint32_t *d_step, fl
                  cudaStream_t s);
 // *err = 1 if a dependency wait of a launch since the plan was built gave up (synchronises s)
 cudaError_t step_read_error(const StepPlan &P, int *err, cudaStream_t s);
-// per-process cache of the autotuned candidate for a class mix on this device (-1: none)
-int step_plan_cached(const std::vector<ClassGeom> &geoms);
+// per-process cache of the autotuned candidate for a class mix on this device (-1: per-pass launches)
+bool step_plan_cached(const std::vector<ClassGeom> &geoms, int *candidate);
 void step_plan_remember(const std::vector<ClassGeom> &geoms, int candidate);

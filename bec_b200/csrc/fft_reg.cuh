@@ -14,6 +14,7 @@
 #include <utility>
 
 #include "common.cuh"
+#include "twiddle_fp32.h"
 
 namespace fftreg {
 
@@ -109,29 +110,37 @@ __device__ __forceinline__ void bfly_s(float2 &x0, float2 &x1, float2 e, float2 
 }
 
 // the butterfly of twiddle w = e^{-+2 pi i K / N} (sign - forward, + when INV)
-template <int K, int N, bool INV>
+// UNIT: the factors of modulus closest to 1 (twiddle_fp32.h; the real-time passes, where a modulus error
+// drains the norm at every step), else the nearest FP32 factors (the imaginary-time passes, which
+// renormalise at every step and gain nothing from the modulus)
+template <int K, int N, bool INV, bool UNIT = true>
 __device__ __forceinline__ void bfly_w(float2 &x0, float2 &x1, float2 e, float2 o)
 {
     constexpr double c = cos_2pi(K, N), s = INV ? sin_2pi(K, N) : -sin_2pi(K, N);
-    if constexpr ((c < 0 ? -c : c) >= (s < 0 ? -s : s)) bfly_c(x0, x1, e, o, (float)c, (float)(s / c));
-    else bfly_s(x0, x1, e, o, (float)s, (float)(c / s));
+    if constexpr ((c < 0 ? -c : c) >= (s < 0 ? -s : s)) {
+        constexpr Twid t = UNIT ? unit_fr(c, s / c) : Twid{(float)c, (float)(s / c)};
+        bfly_c(x0, x1, e, o, t.a, t.b);
+    } else {
+        constexpr Twid t = UNIT ? unit_fr(s, c / s) : Twid{(float)s, (float)(c / s)};
+        bfly_s(x0, x1, e, o, t.a, t.b);
+    }
 }
-template <int K, int N, bool INV>
+template <int K, int N, bool INV, bool UNIT = true>
 __device__ __forceinline__ void bfly_w(float4 &x0, float4 &x1, float4 e, float4 o)
 {
     float2 a0, a1, b0, b1;
-    bfly_w<K, N, INV>(a0, a1, make_float2(e.x, e.y), make_float2(o.x, o.y));
-    bfly_w<K, N, INV>(b0, b1, make_float2(e.z, e.w), make_float2(o.z, o.w));
+    bfly_w<K, N, INV, UNIT>(a0, a1, make_float2(e.x, e.y), make_float2(o.x, o.y));
+    bfly_w<K, N, INV, UNIT>(b0, b1, make_float2(e.z, e.w), make_float2(o.z, o.w));
     x0 = make_float4(a0.x, a0.y, b0.x, b0.y);
     x1 = make_float4(a1.x, a1.y, b1.x, b1.y);
 }
 
 // ---- DFT ---------------------------------------------------------------------
-// x[k] <- sum_n x[n] exp(-+2 pi i n k / N) (sign - forward, + when INV), unnormalised.
-template <int N, bool INV, typename T>
+// x[k] <- sum_n x[n] exp(-+2 pi i n k / N) (sign - forward, + when INV), unnormalised; UNIT as bfly_w.
+template <int N, bool INV, bool UNIT = true, typename T>
 __device__ __forceinline__ void dft(T *x);
 
-template <int N, bool INV, int K, typename T>
+template <int N, bool INV, bool UNIT, int K, typename T>
 __device__ __forceinline__ void combine_one(T *x, const T *e, const T *o)
 {
     if constexpr (K == 0 || 4 * K == N) {
@@ -139,17 +148,17 @@ __device__ __forceinline__ void combine_one(T *x, const T *e, const T *o)
         x[K] = add(e[K], t);
         x[K + N / 2] = sub(e[K], t);
     } else {
-        bfly_w<K, N, INV>(x[K], x[K + N / 2], e[K], o[K]);
+        bfly_w<K, N, INV, UNIT>(x[K], x[K + N / 2], e[K], o[K]);
     }
 }
 
-template <int N, bool INV, typename T, int... K>
+template <int N, bool INV, bool UNIT, typename T, int... K>
 __device__ __forceinline__ void combine_all(T *x, const T *e, const T *o, std::integer_sequence<int, K...>)
 {
-    (combine_one<N, INV, K>(x, e, o), ...);
+    (combine_one<N, INV, UNIT, K>(x, e, o), ...);
 }
 
-template <int N, bool INV, typename T>
+template <int N, bool INV, bool UNIT, typename T>
 __device__ __forceinline__ void dft(T *x)
 {
     if constexpr (N == 1) {
@@ -165,9 +174,9 @@ __device__ __forceinline__ void dft(T *x)
             e[k] = x[2 * k];
             o[k] = x[2 * k + 1];
         }
-        dft<N / 2, INV>(e);
-        dft<N / 2, INV>(o);
-        combine_all<N, INV>(x, e, o, std::make_integer_sequence<int, N / 2>{});
+        dft<N / 2, INV, UNIT>(e);
+        dft<N / 2, INV, UNIT>(o);
+        combine_all<N, INV, UNIT>(x, e, o, std::make_integer_sequence<int, N / 2>{});
     }
 }
 

@@ -4,6 +4,8 @@
 // (propagate, programs/bec_wigner_3d.cuda/wigner.cu:178-199) and the same stored representation.
 // A steady step of the fast classes runs instead as one launch of the fused step kernel
 // (step_kernel.cu); these kernels serve the steps that observe, and the launch-per-pass schedule.
+#include <algorithm>
+
 #include "engine.h"
 #include "step_bodies.cuh"
 
@@ -41,16 +43,38 @@ template <int NZ, bool OBS>
 __global__ void __launch_bounds__(NZ) k_pencil(float4 *__restrict__ state, int nx, int lx, int ny, int cells,
                                                int tiles, const GroupParamsF *__restrict__ gp,
                                                const int *__restrict__ tgroup, const float2 *__restrict__ tw_g,
-                                               PencilArgs pa, double *__restrict__ obs, float inv_out_scale)
+                                               PencilArgs pa, double *__restrict__ obs, float inv_out_scale,
+                                               const float2 *__restrict__ kin)
 {
     extern __shared__ float4 dyn[];
     stepk::pencil_body<NZ, OBS>(VBlock{(int)threadIdx.x, (int)blockIdx.x, 0, NZ}, state, nx, lx, ny, cells, tiles,
-                                gp, tgroup, tw_g, pa, obs, inv_out_scale, dyn);
+                                gp, tgroup, tw_g, pa, obs, inv_out_scale, kin, dyn);
+}
+
+__global__ void k_kin_tables(float2 *__restrict__ tab, const GroupParamsF *__restrict__ gp,
+                             const int *__restrict__ tgroup, int nx, int ny, int nz, int lx, int n_traj, float frac)
+{
+    const int per = nz + nx * ny;
+    const size_t n = (size_t)n_traj * per;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        const int t = (int)(idx / per), i = (int)(idx - (size_t)t * per);
+        const GroupParamsF &P = gp[tgroup[t]];
+        double turns;
+        if (i < nz) {
+            const int iz = kidx(i, nz);
+            turns = P.kin_z * (double)(iz * iz);
+        } else {
+            const int pen = i - nz;
+            const int ix = kidx(pen & (nx - 1), nx), iy = ny > 1 ? kidx(pen >> lx, ny) : 0;
+            turns = P.kin_x * (double)(ix * ix) + P.kin_y * (double)(iy * iy);
+        }
+        tab[idx] = kin_phase(turns * (double)frac);
+    }
 }
 
 template <int NZ, bool OBS>
 void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const float2 *tw,
-                   const PencilArgs &pa, double *obs, float inv_out_scale, cudaStream_t s)
+                   const PencilArgs &pa, double *obs, float inv_out_scale, const float2 *kin, cudaStream_t s)
 {
     const int tiles = c.nx * c.ny / 16;
     const size_t smem = stepk::pencil_smem_bytes<NZ>();
@@ -60,7 +84,7 @@ void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, co
         attr = true;
     }
     k_pencil<NZ, OBS><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, tgroup, tw,
-                                                         pa, obs, inv_out_scale);
+                                                         pa, obs, inv_out_scale, kin);
     g_launches++;
 }
 
@@ -114,9 +138,19 @@ void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, 
     }
 }
 
+void fp32_kin_tables(float2 *tab, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, float frac,
+                     cudaStream_t s)
+{
+    if (c.n_traj <= 0) return;
+    const size_t n = (size_t)c.n_traj * (c.nz + c.nx * c.ny);
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    k_kin_tables<<<blocks, 256, 0, s>>>(tab, gp, tgroup, c.nx, c.ny, c.nz, c.lx, c.n_traj, frac);
+    g_launches++;
+}
+
 void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
                       const float2 *tw_full, float frac, float scale, const float2 *m, double *obs,
-                      float out_scale, cudaStream_t s)
+                      float out_scale, const float2 *kin, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
     PencilArgs pa{};
@@ -128,16 +162,16 @@ void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp,
     const float inv = 1.0f / out_scale;
     switch (c.nz) {
     case 64:
-        if (obs) launch_pencil<64, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
-        else launch_pencil<64, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        if (obs) launch_pencil<64, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, kin, s);
+        else launch_pencil<64, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, kin, s);
         break;
     case 128:
-        if (obs) launch_pencil<128, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
-        else launch_pencil<128, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        if (obs) launch_pencil<128, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, kin, s);
+        else launch_pencil<128, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, kin, s);
         break;
     case 256:
-        if (obs) launch_pencil<256, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, s);
-        else launch_pencil<256, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, s);
+        if (obs) launch_pencil<256, true>(state, c, gp, tgroup, tw_full, pa, obs, inv, kin, s);
+        else launch_pencil<256, false>(state, c, gp, tgroup, tw_full, pa, nullptr, inv, kin, s);
         break;
     default: break;
     }

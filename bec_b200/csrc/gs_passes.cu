@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(NZ, (NZ == 256 ? 3 : 1)) k_gs_pencil(float2 *_
 #pragma unroll
     for (int m = 0; m < R; ++m) x[m] = g[(size_t)(j + G * m) * plane];
     __syncthreads();
-    dft<R, true>(x);
+    dft<R, true, false>(x);
 #pragma unroll
     for (int k1 = 1; k1 < R; ++k1) {
         const float2 w = tw[j * k1];
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(NZ, (NZ == 256 ? 3 : 1)) k_gs_pencil(float2 *_
 #pragma unroll
         for (int jj = 0; jj < G; ++jj) y[r * G + jj] = buf[(p2 * G + jj) * R + ((q + G * r) ^ (p2 & 15))];
 #pragma unroll
-    for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);
+    for (int r = 0; r < R / G; ++r) dft<G, true, false>(y + r * G);
 
     // propagateKSpaceImaginaryTime (wigner_kernel.cu:128-134): exp(-dt_steady frac k^2/2), real, as the
     // product of its (kx, ky) and kz factors
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(NZ, (NZ == 256 ? 3 : 1)) k_gs_pencil(float2 *_
     }
 
 #pragma unroll
-    for (int r = 0; r < R / G; ++r) dft<G, false>(y + r * G);
+    for (int r = 0; r < R / G; ++r) dft<G, false, false>(y + r * G);
 #pragma unroll
     for (int r = 0; r < R / G; ++r)
 #pragma unroll
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(NZ, (NZ == 256 ? 3 : 1)) k_gs_pencil(float2 *_
     __syncthreads();
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[(p * G + j) * R + (k1 ^ (p & 15))];
-    dft<R, false>(x);
+    dft<R, false, false>(x);
 #pragma unroll
     for (int m = 0; m < R; ++m) g[(size_t)(j + G * m) * plane] = x[m];
 }
@@ -192,8 +192,8 @@ __global__ void __launch_bounds__(128) k_gs_plane(float2 *__restrict__ state, in
     const int p_end = (MODE == 2) ? 2 : 4;
 #pragma unroll 1
     for (int pass = p_begin; pass < p_end; ++pass) {
-        if (pass >= 2) dft<N, true>(v);
-        else dft<N, false>(v);
+        if (pass >= 2) dft<N, true, false>(v);
+        else dft<N, false, false>(v);
         if (pass == 0) {
 #pragma unroll
             for (int y = 0; y < N; ++y) s[y * N + (c ^ (y & SW))] = v[y];

@@ -141,3 +141,15 @@ __device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4
     out1 = loss_noise_apply(out1, v1, K, w.b);
 }
 
+
+// The loss-noise increments of four consecutive cells cell0 .. cell0 + 3 of the same trajectory and step:
+// one interleaved group of four Philox4x32-10 draws.
+__device__ __forceinline__ void loss_noise_cell4(float4 out[4], const float4 v0[4], const CellConsts &K, uint32_t k0,
+                                                 uint32_t k1, uint32_t traj, uint32_t step, uint32_t cell0)
+{
+    const u32x4x4 w = philox4x32_10_x4(cell0, step, traj, RNG_TAG_LOSS, k0, k1);
+    out[0] = loss_noise_apply(out[0], v0[0], K, w.a);
+    out[1] = loss_noise_apply(out[1], v0[1], K, w.b);
+    out[2] = loss_noise_apply(out[2], v0[2], K, w.c);
+    out[3] = loss_noise_apply(out[3], v0[3], K, w.d);
+}

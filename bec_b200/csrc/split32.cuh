@@ -29,8 +29,9 @@ __device__ __forceinline__ T w32(T v)
     } else if constexpr (K == 8) {
         return INV ? fftreg::mul_posi(v) : fftreg::mul_negi(v);
     } else {
-        constexpr float c = (float)fftreg::cos_2pi(K, 32), sn = (float)fftreg::sin_2pi(K, 32);
-        return fftreg::cmulc(v, c, INV ? sn : -sn);
+        constexpr fftreg::Twid t =
+            fftreg::unit_cs(fftreg::cos_2pi(K, 32), INV ? fftreg::sin_2pi(K, 32) : -fftreg::sin_2pi(K, 32));
+        return fftreg::cmulc(v, t.a, t.b);
     }
 }
 

@@ -102,18 +102,19 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
             const uint32_t tl = (uint32_t)tlocal[traj];
             const CellConsts K = cell_consts(P);
             const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
-            // cells in pairs: the two Philox draws interleave (loss_noise_cell2)
+            // cells in fours: the four Philox draws interleave (loss_noise_cell4)
 #pragma unroll 1
-            for (int x = 0; x < N; x += 2) {
-                const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
-                float4 *s0 = s + c * N + (x ^ (c & 7)), *s1 = s + c * N + ((x + 1) ^ (c & 7));
-                const float4 v0 = *s0, v1 = *s1;
-                float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
-                float4 o1 = nonlinear_cell(v1, 0.5f * (X1 * X1 + base), K);
-                if (P.noise)
-                    loss_noise_cell2(o0, v0, o1, v1, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
-                *s0 = o0;
-                *s1 = o1;
+            for (int x = 0; x < N; x += 4) {
+                float4 v0[4], o[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float X = -P.xmax + P.dx * (float)(x + q);
+                    v0[q] = s[c * N + ((x + q) ^ (c & 7))];
+                    o[q] = nonlinear_cell(v0[q], 0.5f * (X * X + base), K);
+                }
+                if (P.noise) loss_noise_cell4(o, v0, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) s[c * N + ((x + q) ^ (c & 7))] = o[q];
             }
 #pragma unroll
             for (int x = 0; x < N; ++x) v[x] = s[c * N + (x ^ (c & 7))];
@@ -176,7 +177,8 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
         const uint32_t tl = (uint32_t)tlocal[traj];
         const CellConsts K = cell_consts(P);
         const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
-        // cells in pairs (x, x + 1; kblk keeps pairs of even s adjacent): the two Philox draws interleave
+        // cells in pairs (x, x + 1; kblk keeps pairs of even s adjacent): the two Philox draws interleave.
+        // (Fours measured slower here: the larger loop body misses in the instruction cache.)
 #pragma unroll 1
         for (int s = 0; s < 16; s += 2) {
             const int x = kblk(s, h);
@@ -213,6 +215,14 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
 }
 
 // ---------------------------------------------------------------- pencil pass
+// 8-byte global -> shared copy that completes asynchronously (cp.async), and the wait for this thread's copies
+__device__ __forceinline__ void copy_async8(float2 *dst_smem, const float2 *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 struct PencilArgs {
     float frac;          // kick in units of dt (0.5 + 0.5 for a full step)
     float scale;         // 1/cells times the output scale
@@ -234,9 +244,10 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
                                             int cells, int tiles, const GroupParamsF *__restrict__ gp,
                                             const int *__restrict__ tgroup, const float2 *__restrict__ tw_g,
                                             const PencilArgs &pa, double *__restrict__ obs, float inv_out_scale,
-                                            float4 *dyn)
+                                            const float2 *__restrict__ kin, float4 *dyn)
 {
     constexpr int R = 16, G = NZ / 16;
+    (void)gp; (void)tgroup; (void)lx;
     float4 *buf = dyn;                                          // 16 pencils x NZ
     float2 *tw = reinterpret_cast<float2 *>(dyn + 16 * NZ);     // W_NZ^e, e < NZ
     float2 *kzp = tw + NZ;                                      // kz phase
@@ -245,19 +256,21 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
     const int t = vb.tid;
     const int traj = vb.bid / tiles;
     const int pen0 = (vb.bid - traj * tiles) * 16;
-    const GroupParamsF P = gp[tgroup[traj]];
     const int plane = nx * ny;
 
-    for (int i = t; i < NZ; i += NZ) {
-        tw[i] = tw_g[i];
-        const int iz = kidx(i, NZ);
-        kzp[i] = kin_phase(P.kin_z * (double)(iz * iz) * (double)pa.frac);     // e^{+i kz^2/2 dt frac}
-    }
-    if (t < 16) {
-        const int pen = pen0 + t;
-        const int ix = kidx(pen & (nx - 1), nx), iy = ny > 1 ? kidx(pen >> lx, ny) : 0;
-        const float2 e = kin_phase((P.kin_x * (double)(ix * ix) + P.kin_y * (double)(iy * iy)) * (double)pa.frac);
-        kxyp[t] = make_float2(pa.scale * e.x, pa.scale * e.y);
+    // kinetic phase e^{+i k^2/2 dt frac} (wigner_kernel.cu:137-151) as the product of the per-kz and the
+    // per-pencil factors, from the class's table for this kick fraction (fp32_kin_tables); kin == NULL
+    // means frac == 0, no kick. Thread t fills entry t of the twiddle and kz tables (NZ threads).
+    // The table entries go to shared memory by asynchronous copies, so the state loads below issue at once
+    // and no register holds a table value in between.
+    const float2 *kt = kin ? kin + (size_t)traj * (NZ + plane) : nullptr;
+    copy_async8(tw + t, tw_g + t);
+    if (kt) {
+        copy_async8(kzp + t, kt + t);
+        if (t < 16) copy_async8(kxyp + t, kt + NZ + pen0 + t);
+    } else {
+        kzp[t] = make_float2(1.f, 0.f);
+        if (t < 16) kxyp[t] = make_float2(1.f, 0.f);
     }
 
     // stage 1: thread (p, j) holds z = j + G m, m < 16
@@ -266,6 +279,8 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
     float4 x[R];
 #pragma unroll
     for (int m = 0; m < R; ++m) x[m] = g[(size_t)(j + G * m) * plane];
+    copy_async_wait();
+    if (t < 16) kxyp[t] = make_float2(pa.scale * kxyp[t].x, pa.scale * kxyp[t].y);
     vb.sync();                                                  // tables ready
     dft<R, true>(x);                                            // over m -> k1 (inverse)
 #pragma unroll
@@ -287,13 +302,16 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
 #pragma unroll
     for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);   // over j -> k2: k = k1 + 16 k2
 
+    // the two unit-modulus factors are applied to the data one after the other: their product, the same
+    // every step for a mode, would round the same way every step and drift the norm of the most
+    // populated modes coherently
     const float2 pxy = kxyp[p2];
 #pragma unroll
     for (int r = 0; r < R / G; ++r)
 #pragma unroll
         for (int k2 = 0; k2 < G; ++k2) {
             const int k = q + G * r + R * k2;
-            float4 v = fftreg::cmulw(y[r * G + k2], cmul(pxy, kzp[k]));
+            float4 v = fftreg::cmulw(fftreg::cmulw(y[r * G + k2], pxy), kzp[k]);
             if (pa.has_m) {
                 const float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
                 const float2 an = cadd(cmul(pa.m[0], a), cmul(pa.m[1], b));

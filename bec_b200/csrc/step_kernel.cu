@@ -17,7 +17,9 @@
 // The list is longest-first (the classes by cells per trajectory, the largest first) and
 // interleaved: a trajectory's plane items follow its pencil items at a distance of `lead` items.
 // CTAs take items in list order with one atomic ticket each, so a waiting plane item only waits for
-// items that running CTAs took before it, and no wait can depend on a CTA that has not started. The
+// items that running CTAs took before it, and no wait can depend on a CTA that has not started. (A CTA
+// takes its next ticket once its current item is past its wait; the current item then completes, so a
+// ticket held that way is always started.) The
 // interleave lets memory-bound pencil items run beside issue-bound plane items, and a trajectory's
 // plane items read what its pencil items wrote while it is still in L2. The last CTA to finish resets
 // the counters and advances the Philox step index, so every launch is identical and a captured CUDA
@@ -77,8 +79,9 @@ __device__ __forceinline__ void run_pencil(const StepClassDev &c, const GroupPar
     p.scale = 1.0f / (float)c.cells;        // exact: cells is a power of two
     const VBlock vb{(int)threadIdx.x % NZ, traj * c.tiles + sub * VB + v, VB == 1 ? 0 : 1 + v, NZ};
     float4 *dyn = smem + v * (stepk::pencil_smem_bytes<NZ>() / sizeof(float4));
+    const float2 *kin = pa.frac == 1.0f ? c.kin[1] : pa.frac == 0.5f ? c.kin[0] : nullptr;
     stepk::pencil_body<NZ, false>(vb, c.state, c.nx, c.lx, c.ny, c.cells, c.tiles, gp, c.tgroup, c.tw, p, nullptr,
-                                  1.0f, dyn);
+                                  1.0f, kin, dyn);
 }
 
 template <int N>
@@ -108,9 +111,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(StepLaunch L, PencilArgs p
     __shared__ int4 s_item;
     __shared__ int s_last;
     const uint32_t step = *L.d_step;
+    // thread 0 holds the ticket of the CTA's next item, taken while the current one runs, so the
+    // atomic's round trip stays off the item-to-item path
+    int next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
     for (;;) {
         if (threadIdx.x == 0) {
-            const int k = atomicAdd(L.queue, 1);
+            const int k = next;
             int4 it = make_int4(-1, 0, 0, 0);
             if (k < L.n_items) {
                 it = L.items[k];
@@ -130,6 +137,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(StepLaunch L, PencilArgs p
                 }
             }
             s_item = it;
+            if (it.x >= 0) next = atomicAdd(L.queue, 1);
         }
         __syncthreads();
         const int4 it = s_item;
@@ -216,7 +224,7 @@ const char *step_plan_name(int candidate)
 {
     static const char *names[] = {"two-phase", "interleave 0.5 wave", "interleave 1 wave", "interleave 2 waves",
                                   "interleave 4 waves"};
-    return candidate >= 0 && candidate < kStepCandidates ? names[candidate] : "unfused";
+    return candidate >= 0 && candidate < kStepCandidates ? names[candidate] : "per-pass launches";
 }
 
 cudaError_t step_plan_build(StepPlan &P, const std::vector<ClassGeom> &geoms, const std::vector<StepClassDev> &cls,
@@ -355,12 +363,14 @@ cudaError_t step_read_error(const StepPlan &P, int *err, cudaStream_t s)
     return e;
 }
 
-int step_plan_cached(const std::vector<ClassGeom> &geoms)
+bool step_plan_cached(const std::vector<ClassGeom> &geoms, int *candidate)
 {
     PlanKey k = plan_key(geoms);
     std::lock_guard<std::mutex> lock(g_plan_mutex);
     auto it = g_plan_cache.find(k);
-    return it == g_plan_cache.end() ? -1 : it->second;
+    if (it == g_plan_cache.end()) return false;
+    *candidate = it->second;
+    return true;
 }
 
 void step_plan_remember(const std::vector<ClassGeom> &geoms, int candidate)

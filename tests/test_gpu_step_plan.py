@@ -54,31 +54,43 @@ def test_every_schedule_gives_the_same_bits(monkeypatch, ground_states):
     for plan in ["0", "1", "2", "3", "4", None]:
         got = _run(monkeypatch, plan, ground_states)
         p = got["plan"]
-        assert p["fused_classes"] == 4                     # every class but the 2D slice
         if plan is None:
-            assert p["chosen"] in ("autotuned", "cached") and 0 <= p["candidate"] < 5
+            assert p["chosen"] in ("autotuned", "cached") and -1 <= p["candidate"] < 5
         else:
             assert p["chosen"] == "forced" and p["candidate"] == int(plan)
+        assert p["fused_classes"] == (4 if p["candidate"] >= 0 else 0)   # every class but the 2D slice
         np.testing.assert_array_equal(got["mom"], ref["mom"])
         np.testing.assert_array_equal(got["now"], ref["now"])
         for a, b in zip(got["states"], ref["states"]):
             np.testing.assert_array_equal(a, b)
 
 
-def test_autotuner_reports_timings_and_one_launch_per_step(monkeypatch, ground_states):
-    monkeypatch.delenv("BEC_STEP_PLAN", raising=False)
+def _three_classes(ground_states):
     groups = [GROUPS[0], GROUPS[1], GROUPS[2]]
     eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
     for g in range(3):
         eng.init_group(g, ground_states[g])
     eng.start_evolution()
     eng.evolve(3)
+    return eng, groups
+
+
+def test_autotuner_reports_timings(monkeypatch, ground_states):
+    monkeypatch.delenv("BEC_STEP_PLAN", raising=False)
+    eng, _ = _three_classes(ground_states)
     p = eng.step_plan
     assert p["chosen"] in ("autotuned", "cached")
     if p["chosen"] == "autotuned":
-        ms = p["candidate_ms_per_step"]
-        assert len(ms) == 5 and all(v > 0 for v in ms)
-        assert ms[p["candidate"]] == min(ms)
+        ms = p["candidate_ms_per_step"]           # per-pass launches, then the fused candidates 0..4
+        assert len(ms) == 6 and all(v > 0 for v in ms)
+        assert ms[p["candidate"] + 1] == min(ms)
+
+
+def test_fused_plan_is_one_launch_per_step(monkeypatch, ground_states):
+    monkeypatch.setenv("BEC_STEP_PLAN", "2")
+    eng, groups = _three_classes(ground_states)
+    p = eng.step_plan
+    assert p["chosen"] == "forced" and p["fused_classes"] == 3
     eng.evolve(64)                                 # steady steps: captured graph replays
     assert eng.step_graphs == 2
     assert eng.last_launch_count == 64 * p["launches_per_step"] + 1   # + the step index write
