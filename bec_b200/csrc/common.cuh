@@ -68,6 +68,14 @@ BEC_HD u32x4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, u
     return u32x4{c0, c1, c2, c3};
 }
 
+// hi and lo words of the 64-bit product a * b (one 32 x 32 -> 64 multiply)
+__device__ __forceinline__ void mul_wide(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo)
+{
+    const uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
 // Two Philox4x32-10 draws under one key, their rounds interleaved: the two multiply chains are
 // independent, so each hides the other's latency, and the key schedule is computed once.
 struct u32x4x2 { u32x4 a, b; };
@@ -78,10 +86,11 @@ __device__ __forceinline__ u32x4x2 philox4x32_10_x2(uint32_t a0, uint32_t a1, ui
 {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t la0 = 0xD2511F53u * a0, ha0 = __umulhi(0xD2511F53u, a0);
-        const uint32_t la1 = 0xCD9E8D57u * a2, ha1 = __umulhi(0xCD9E8D57u, a2);
-        const uint32_t lb0 = 0xD2511F53u * b0, hb0 = __umulhi(0xD2511F53u, b0);
-        const uint32_t lb1 = 0xCD9E8D57u * b2, hb1 = __umulhi(0xCD9E8D57u, b2);
+        uint32_t la0, ha0, la1, ha1, lb0, hb0, lb1, hb1;
+        mul_wide(0xD2511F53u, a0, ha0, la0);
+        mul_wide(0xCD9E8D57u, a2, ha1, la1);
+        mul_wide(0xD2511F53u, b0, hb0, lb0);
+        mul_wide(0xCD9E8D57u, b2, hb1, lb1);
         a0 = ha1 ^ a1 ^ k0; a2 = ha0 ^ a3 ^ k1; a1 = la1; a3 = la0;
         b0 = hb1 ^ b1 ^ k0; b2 = hb0 ^ b3 ^ k1; b1 = lb1; b3 = lb0;
         k0 += 0x9E3779B9u;
@@ -103,14 +112,15 @@ __device__ __forceinline__ u32x4x4 philox4x32_10_x4(uint32_t c0, uint32_t c1, ui
     uint32_t d0 = c0 + 3u, d1 = c1, d2 = c2, d3 = c3;
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t la0 = 0xD2511F53u * a0, ha0 = __umulhi(0xD2511F53u, a0);
-        const uint32_t la1 = 0xCD9E8D57u * a2, ha1 = __umulhi(0xCD9E8D57u, a2);
-        const uint32_t lb0 = 0xD2511F53u * b0, hb0 = __umulhi(0xD2511F53u, b0);
-        const uint32_t lb1 = 0xCD9E8D57u * b2, hb1 = __umulhi(0xCD9E8D57u, b2);
-        const uint32_t le0 = 0xD2511F53u * e0, he0 = __umulhi(0xD2511F53u, e0);
-        const uint32_t le1 = 0xCD9E8D57u * e2, he1 = __umulhi(0xCD9E8D57u, e2);
-        const uint32_t ld0 = 0xD2511F53u * d0, hd0 = __umulhi(0xD2511F53u, d0);
-        const uint32_t ld1 = 0xCD9E8D57u * d2, hd1 = __umulhi(0xCD9E8D57u, d2);
+        uint32_t la0, ha0, la1, ha1, lb0, hb0, lb1, hb1, le0, he0, le1, he1, ld0, hd0, ld1, hd1;
+        mul_wide(0xD2511F53u, a0, ha0, la0);
+        mul_wide(0xCD9E8D57u, a2, ha1, la1);
+        mul_wide(0xD2511F53u, b0, hb0, lb0);
+        mul_wide(0xCD9E8D57u, b2, hb1, lb1);
+        mul_wide(0xD2511F53u, e0, he0, le0);
+        mul_wide(0xCD9E8D57u, e2, he1, le1);
+        mul_wide(0xD2511F53u, d0, hd0, ld0);
+        mul_wide(0xCD9E8D57u, d2, hd1, ld1);
         a0 = ha1 ^ a1 ^ k0; a2 = ha0 ^ a3 ^ k1; a1 = la1; a3 = la0;
         b0 = hb1 ^ b1 ^ k0; b2 = hb0 ^ b3 ^ k1; b1 = lb1; b3 = lb0;
         e0 = he1 ^ e1 ^ k0; e2 = he0 ^ e3 ^ k1; e1 = le1; e3 = le0;

@@ -77,34 +77,49 @@ __device__ __forceinline__ float2 cis_taylor(float t)
 
 __device__ __forceinline__ float exp_taylor(float x) { return fmaf(x, fmaf(x, fmaf(x, 1.f / 6.f, 0.5f), 1.f), 1.f); }
 
+// The substep's factors da, db from the midpoint estimate (xa, xb).
+__device__ __forceinline__ void nonlinear_factors(float2 xa, float2 xb, float hV, float hVd, const CellConsts &K,
+                                                  float2 &da, float2 &db)
+{
+    const float na = xa.x * xa.x + xa.y * xa.y;
+    const float nb = xb.x * xb.x + xb.y * xb.y;
+    const float ra = fmaf(K.hl111 * na, na, K.hl12 * nb);
+    const float rb = fmaf(K.hl22, nb, K.hl12 * na);
+    const float ta = fmaf(K.hg11, na, fmaf(K.hg12, nb, hV));
+    const float tb = fmaf(K.hg22, nb, fmaf(K.hg12, na, hVd));
+    float2 ea, eb;
+    float ma, mb;
+    if (fmaxf(fabsf(ta), fabsf(tb)) <= 0.5f && fmaxf(fabsf(ra), fabsf(rb)) <= 0.015625f) {
+        ea = cis_taylor(ta);
+        eb = cis_taylor(tb);
+        ma = exp_taylor(ra);
+        mb = exp_taylor(rb);
+    } else {
+        sincosf(ta, &ea.y, &ea.x);
+        sincosf(tb, &eb.y, &eb.x);
+        ma = expf(ra);
+        mb = expf(rb);
+    }
+    da = make_float2(ma * ea.x, ma * ea.y);
+    db = make_float2(mb * eb.x, mb * eb.y);
+}
+
 // One cell: v = (a, b) at the start of the substep, V the trap potential.
 __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const CellConsts &K)
 {
     const float2 a0 = make_float2(v.x, v.y), b0 = make_float2(v.z, v.w);
     const float hV = V * K.hdt, hVd = hV - K.hdet;
-    float2 xa = a0, xb = b0, da = make_float2(0.f, 0.f), db = make_float2(0.f, 0.f);
+    float2 da, db;
+    if (K.itmax == 1) {
+        // one midpoint iteration (every workload here): the factors of the start values, applied twice
+        nonlinear_factors(a0, b0, hV, hVd, K, da, db);
+        const float2 ao = cmul(cmul(a0, da), da), bo = cmul(cmul(b0, db), db);
+        return make_float4(ao.x, ao.y, bo.x, bo.y);
+    }
+    float2 xa = a0, xb = b0;
+    da = db = make_float2(0.f, 0.f);
     for (int it = 0; it < K.itmax; ++it) {
-        const float na = xa.x * xa.x + xa.y * xa.y;
-        const float nb = xb.x * xb.x + xb.y * xb.y;
-        const float ra = fmaf(K.hl111 * na, na, K.hl12 * nb);
-        const float rb = fmaf(K.hl22, nb, K.hl12 * na);
-        const float ta = fmaf(K.hg11, na, fmaf(K.hg12, nb, hV));
-        const float tb = fmaf(K.hg22, nb, fmaf(K.hg12, na, hVd));
-        float2 ea, eb;
-        float ma, mb;
-        if (fmaxf(fabsf(ta), fabsf(tb)) <= 0.5f && fmaxf(fabsf(ra), fabsf(rb)) <= 0.015625f) {
-            ea = cis_taylor(ta);
-            eb = cis_taylor(tb);
-            ma = exp_taylor(ra);
-            mb = exp_taylor(rb);
-        } else {
-            sincosf(ta, &ea.y, &ea.x);
-            sincosf(tb, &eb.y, &eb.x);
-            ma = expf(ra);
-            mb = expf(rb);
-        }
-        da = make_float2(ma * ea.x, ma * ea.y);
-        db = make_float2(mb * eb.x, mb * eb.y);
+        nonlinear_factors(xa, xb, hV, hVd, K, da, db);
         xa = cmul(a0, da);
         xb = cmul(b0, db);
     }

@@ -687,6 +687,20 @@ int oracle_pulse(oracle_ens *e, double theta, double phi)
     return BEC_OK;
 }
 
+/* Rounds every stored amplitude to FP32 and back (no reference counterpart): a perturbation of FP32
+ * rounding size, applied after every step of a second oracle run, shows how far rounding alone moves
+ * the trajectories of a configuration. */
+int oracle_round_fp32(oracle_ens *e)
+{
+    if (!e || !e->initialised) return BEC_ERR_STATE;
+    size_t n = (size_t)e->d.cells * e->d.ne;
+    for (size_t i = 0; i < n; i++) {
+        e->a[i] = (double)(float)creal(e->a[i]) + I * (double)(float)cimag(e->a[i]);
+        e->b[i] = (double)(float)creal(e->b[i]) + I * (double)(float)cimag(e->b[i]);
+    }
+    return BEC_OK;
+}
+
 /* initEvolution's tail (wigner.cu:222-225): equilibration steps, then pi/2. */
 int oracle_start_evolution(oracle_ens *e, int threads)
 {

@@ -46,6 +46,7 @@ void oracle_free(oracle_ens *e);
 int oracle_init(oracle_ens *e, const double *psi_gs, const double *noise);
 int oracle_evolve(oracle_ens *e, int n_steps, int threads);
 int oracle_pulse(oracle_ens *e, double theta, double phi);
+int oracle_round_fp32(oracle_ens *e);
 int oracle_start_evolution(oracle_ens *e, int threads);
 int oracle_moments(oracle_ens *e, bec_moments *out);
 int oracle_traj_moments(oracle_ens *e, bec_moments *out);

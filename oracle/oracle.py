@@ -55,6 +55,7 @@ def lib():
         L.oracle_init.argtypes = [C.c_void_p, dp, dp]
         L.oracle_evolve.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oracle_pulse.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.oracle_round_fp32.argtypes = [C.c_void_p]
         L.oracle_start_evolution.argtypes = [C.c_void_p, C.c_int]
         L.oracle_moments.argtypes = [C.c_void_p, P(BecMoments)]
         L.oracle_traj_moments.argtypes = [C.c_void_p, P(BecMoments)]
@@ -179,6 +180,10 @@ class OracleEnsemble:
 
     def pulse(self, theta, phi=0.0):
         _check(lib().oracle_pulse(self._h, theta, phi), "pulse")
+
+    def round_fp32(self):
+        """Rounds the stored state to FP32 and back (a rounding-size perturbation)."""
+        _check(lib().oracle_round_fp32(self._h), "round_fp32")
 
     def start_evolution(self, threads=0):
         _check(lib().oracle_start_evolution(self._h, threads), "start_evolution")

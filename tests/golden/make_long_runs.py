@@ -14,10 +14,13 @@ the fixtures are reproducible bit for bit on any machine with the same libm:
       steps, axial profiles every 2500 steps; at the end the final pi/2 about
       50 axis angles alpha_j = 2 pi j / 50, evaluated literally
       (halfPiRotate + reduce, wigner_kernel.cu:344-360, wigner.cu:257-265).
+  spin_echo_32x32x256_4traj_fp32round.npz  the same run with the stored state rounded to FP32 after
+      every step: how far FP32 rounding alone moves this configuration's trajectories and ensemble
+      observables (at N = 70000 the trajectories part within about 2000 steps).
 
-    python tests/golden/make_long_runs.py [--only ensemble|spin_echo] [--threads N]
+    python tests/golden/make_long_runs.py [--only ensemble|spin_echo|spin_echo_fp32round] [--threads N]
 
-The spin echo takes about an hour of four host cores.
+Each spin echo takes about an hour of four host cores.
 """
 import argparse
 import json
@@ -35,7 +38,7 @@ GS_STEPS = 2000
 N_PHASE = 50
 
 
-def _run(p, steps, sample_every, axial_every, pi_pulse_step, threads, log):
+def _run(p, steps, sample_every, axial_every, pi_pulse_step, threads, log, round_fp32=False):
     from bec_b200._abi import BEC_GS_FIXED_STEPS
     from bec_b200.configs import copy_params
     from oracle import oracle as O
@@ -49,6 +52,8 @@ def _run(p, steps, sample_every, axial_every, pi_pulse_step, threads, log):
     mom, traj, axial, axial_steps = [], [], [], []
     for i in range(1, steps + 1):
         e.evolve(1, threads)
+        if round_fp32:
+            e.round_fp32()
         if i % sample_every == 0:
             mom.append(e.moments())
             traj.append(e.traj_moments())
@@ -85,14 +90,23 @@ def spin_echo(threads, log):
     return "spin_echo_32x32x256_4traj.npz", meta, out
 
 
+def spin_echo_fp32round(threads, log):
+    from bec_b200.configs import spin_echo_32x32x256
+    p = spin_echo_32x32x256(ne=4, seed=4)
+    meta = dict(params="spin_echo_32x32x256(ne=4, seed=4)", gs_steps=GS_STEPS, steps=25000, sample_every=500,
+                axial_every=2500, pi_pulse_step=12500, perturbation="state rounded to FP32 after every step")
+    out = _run(p, 25000, 500, 2500, 12500, threads, log, round_fp32=True)
+    return "spin_echo_32x32x256_4traj_fp32round.npz", meta, out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["ensemble", "spin_echo"], default=None)
+    ap.add_argument("--only", choices=["ensemble", "spin_echo", "spin_echo_fp32round"], default=None)
     ap.add_argument("--threads", type=int, default=4)
     a = ap.parse_args()
     from oracle import oracle as O
     O.build()
-    for fn in (ensemble, spin_echo):
+    for fn in (ensemble, spin_echo, spin_echo_fp32round):
         if a.only and fn.__name__ != a.only:
             continue
         name, meta, out = fn(a.threads, lambda m: print(f"[{fn.__name__}] {m}", flush=True))
