@@ -81,7 +81,8 @@ struct bec_ctx {
     bool graphs_failed = false;
     StepPlan plan;                       // batched: the fused step of the register-path classes
     std::vector<char> fused;             // per class: 1 when its passes run in the fused step
-    int plan_mode = -2;                  // -2: not chosen yet, -1: per-pass launches, >= 0: fused candidate
+    int plan_mode = -2;                  // -2: not chosen yet, else the schedule candidate (ensure_plan)
+    int plane_occupancy = 0;             // per-pass plane launches: 0 = 16 warps per SM, 1 = 20
     std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
     long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
@@ -425,7 +426,8 @@ bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *
         const size_t ci = &c - &ctx->classes[0];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
         if (ctx->use_fast && fp32_fast_plane_supported(c.geom)) {
-            fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step, ctx->stream);
+            fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step, ctx->plane_occupancy,
+                            ctx->stream);
         } else {
             float2 *tx, *ty;
             bec_status st;
@@ -464,19 +466,33 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
     return BEC_OK;
 }
 
-// The fused step plan of a batched context, chosen once before its first step. BEC_STEP_PLAN in the
-// environment forces one ("unfused" for launches per pass, or a candidate number 0..4); otherwise a plan
-// cached for the same class mix on this device is reused, or the candidates are timed on a copy of the
-// state (BEC_AUTOTUNE=0 skips the timing and takes the one-wave interleave).
+// The split-step schedule of a batched context, chosen once before its first step. Candidates:
+//   0  per-pass launches, plane passes at 16 warps per SM (no register spill)
+//   1  per-pass launches, plane passes at 20 warps per SM (96 registers, a small spill)
+//   2 + k  the fused step kernel on work list k (two-phase, interleaved at 0.5, 1, 2, 4 waves)
+// BEC_STEP_PLAN in the environment forces one ("unfused" = 0, "unfused-20" = 1, "0".."4" = fused k);
+// otherwise a choice cached for the same class mix on this device is reused, or every candidate is timed
+// on a copy of the state (BEC_AUTOTUNE=0 skips the timing and takes candidate 0).
+constexpr int kPerPassCandidates = 2;
+constexpr int kAllCandidates = kPerPassCandidates + kStepCandidates;
+
+std::string candidate_name(int c)
+{
+    if (c == 0) return "per-pass launches, 16 warps per SM";
+    if (c == 1) return "per-pass launches, 20 warps per SM";
+    return std::string("fused ") + step_plan_name(c - kPerPassCandidates);
+}
+
 bec_status ensure_plan(bec_ctx *ctx)
 {
     if (ctx->path != BEC_PATH_FP32_BATCHED || ctx->plan_mode != -2) return BEC_OK;
     ctx->fused.assign(ctx->classes.size(), 0);
     const char *force = std::getenv("BEC_STEP_PLAN");
+    const std::string fs = force ? force : "";
     std::vector<ClassGeom> geoms;
     std::vector<StepClassDev> devs;
     std::vector<int> offs, idx;
-    if (ctx->use_fast && !(force && std::string(force) == "unfused")) {
+    if (ctx->use_fast) {
         for (size_t ci = 0; ci < ctx->classes.size(); ++ci) {
             ClassRec &c = ctx->classes[ci];
             if (c.geom.n_traj == 0 || !step_class_supported(c.geom)) continue;
@@ -498,23 +514,38 @@ bec_status ensure_plan(bec_ctx *ctx)
             idx.push_back((int)ci);
         }
     }
-    if (geoms.empty()) {
-        ctx->plan_mode = -1;
-        ctx->plan_desc = "{\"plan\": \"unfused\", \"launches_per_step\": \"2 per class\"}";
+    // schedule c: per-pass occupancy / fused work list, no timing
+    auto apply = [&](int c) -> bec_status {
+        if (c < kPerPassCandidates) {
+            ctx->plan.ready = false;
+            ctx->plane_occupancy = c;
+            for (int ci : idx) ctx->fused[ci] = 0;
+            return BEC_OK;
+        }
+        if (step_plan_build(ctx->plan, geoms, devs, offs, c - kPerPassCandidates, ctx->stream) != cudaSuccess)
+            return fail(ctx, BEC_ERR_CUDA, "fused step plan");
+        ctx->plane_occupancy = 0;
+        for (int ci : idx) ctx->fused[ci] = 1;
         return BEC_OK;
-    }
-    // candidates: -1 = two launches per class (per-pass kernels), 0 .. kStepCandidates-1 = fused work lists
-    int cand = 2;
+    };
+    int cand = 0;
     std::string how = "default";
-    std::vector<double> tms(kStepCandidates + 1, -1.0);   // [0]: per-pass launches, [k + 1]: candidate k
-    if (force && *force) {
-        cand = std::atoi(force);
-        if (cand < 0 || cand >= kStepCandidates) return fail(ctx, BEC_ERR_INVALID_ARG, "BEC_STEP_PLAN out of range");
+    std::vector<double> tms(kAllCandidates, -1.0);
+    bec_status st;
+    if (fs == "unfused" || fs == "unfused-20") {
+        cand = fs == "unfused" ? 0 : 1;
+        how = "forced";
+    } else if (!fs.empty()) {
+        const int k = std::atoi(fs.c_str());
+        if (k < 0 || k >= kStepCandidates || geoms.empty())
+            return fail(ctx, BEC_ERR_INVALID_ARG, "BEC_STEP_PLAN: no such fused work list for this context");
+        cand = kPerPassCandidates + k;
         how = "forced";
     } else if (step_plan_cached(geoms, &cand)) {
         how = "cached";
     } else {
         const char *at = std::getenv("BEC_AUTOTUNE");
+        const int n_cand = geoms.empty() ? kPerPassCandidates : kAllCandidates;
         if (!(at && at[0] == '0')) {
             // time every candidate's full step on a copy of the state: the copy (and any pending pulse) is
             // restored afterwards, so tuning changes nothing of the run; every candidate computes the same bits
@@ -530,16 +561,10 @@ bec_status ensure_plan(bec_ctx *ctx)
                 }
                 const bool had_pulse = ctx->has_pulse;
                 ctx->has_pulse = false;
-                bec_status st = BEC_OK;
+                st = BEC_OK;
                 double best = 1e30;
-                for (int k = -1; k < kStepCandidates && st == BEC_OK; ++k) {
-                    if (k < 0) {
-                        ctx->plan.ready = false;
-                    } else if (step_plan_build(ctx->plan, geoms, devs, offs, k, ctx->stream) != cudaSuccess) {
-                        st = fail(ctx, BEC_ERR_CUDA, "fused step plan");
-                        break;
-                    }
-                    for (int ci : idx) ctx->fused[ci] = k >= 0;
+                for (int k = 0; k < n_cand && st == BEC_OK; ++k) {
+                    if ((st = apply(k))) break;
                     for (int r = 0; r < 4 && st == BEC_OK; ++r) {
                         if (r == 1) cudaEventRecord(ctx->ev0, ctx->stream);
                         st = batched_step(ctx, 0.5f, true);
@@ -547,13 +572,13 @@ bec_status ensure_plan(bec_ctx *ctx)
                     if (st) break;
                     cudaEventRecord(ctx->ev1, ctx->stream);
                     if (cudaEventSynchronize(ctx->ev1) != cudaSuccess) {
-                        st = fail(ctx, BEC_ERR_CUDA, std::string("fused step: ") + cudaGetErrorString(cudaGetLastError()));
+                        st = fail(ctx, BEC_ERR_CUDA, std::string("step timing: ") + cudaGetErrorString(cudaGetLastError()));
                         break;
                     }
                     float ms = 0.f;
                     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-                    tms[k + 1] = ms / 3.0;
-                    if (tms[k + 1] < best) { best = tms[k + 1]; cand = k; }
+                    tms[k] = ms / 3.0;
+                    if (tms[k] < best) { best = tms[k]; cand = k; }
                 }
                 o = 0;
                 for (auto &c : ctx->classes) {
@@ -564,7 +589,6 @@ bec_status ensure_plan(bec_ctx *ctx)
                 cudaStreamSynchronize(ctx->stream);
                 cudaFree(save);
                 ctx->has_pulse = had_pulse;
-                std::fill(ctx->fused.begin(), ctx->fused.end(), 0);
                 if (st) return st;
                 int err = 0;
                 CKC(step_read_error(ctx->plan, &err, ctx->stream));
@@ -576,34 +600,27 @@ bec_status ensure_plan(bec_ctx *ctx)
             }
         }
     }
-    char buf[512];
-    std::string t = "[";
-    for (int k = 0; k <= kStepCandidates; ++k) {
-        std::snprintf(buf, sizeof buf, "%s%.4f", k ? ", " : "", tms[k]);
-        t += buf;
-    }
-    t += "]";
-    if (cand < 0) {
-        ctx->plan.ready = false;
-        ctx->plan_mode = -1;
-        std::snprintf(buf, sizeof buf,
-                      "{\"plan\": \"%s\", \"candidate\": -1, \"chosen\": \"%s\", \"fused_classes\": 0, "
-                      "\"launches_per_step\": %d, \"candidate_ms_per_step\": ",
-                      step_plan_name(-1), how.c_str(), 2 * (int)idx.size());
-        ctx->plan_desc = std::string(buf) + t + ", \"candidates\": \"per-pass launches, then fused 0..4\"}";
-        return BEC_OK;
-    }
-    if (step_plan_build(ctx->plan, geoms, devs, offs, cand, ctx->stream) != cudaSuccess)
-        return fail(ctx, BEC_ERR_CUDA, "fused step plan");
+    if ((st = apply(cand))) return st;
     CKC(cudaStreamSynchronize(ctx->stream));
-    for (int ci : idx) ctx->fused[ci] = 1;
     ctx->plan_mode = cand;
-    std::snprintf(buf, sizeof buf,
-                  "{\"plan\": \"%s\", \"candidate\": %d, \"chosen\": \"%s\", \"grid\": %d, \"items\": %d, "
-                  "\"fused_classes\": %d, \"launches_per_step\": %d, \"candidate_ms_per_step\": ",
-                  step_plan_name(cand), cand, how.c_str(), ctx->plan.grid, ctx->plan.n_items, (int)idx.size(),
-                  ctx->plan.two_phase ? 2 : 1);
-    ctx->plan_desc = std::string(buf) + t + ", \"candidates\": \"per-pass launches, then fused 0..4\"}";
+    const bool fused = cand >= kPerPassCandidates;
+    int n_classes = 0;
+    for (auto &c : ctx->classes) n_classes += c.geom.n_traj > 0;
+    char buf[256];
+    std::string j = "{\"plan\": \"" + candidate_name(cand) + "\", \"candidate\": " + std::to_string(cand) +
+                    ", \"chosen\": \"" + how + "\", \"fused_classes\": " + std::to_string(fused ? (int)idx.size() : 0) +
+                    ", \"launches_per_step\": " +
+                    std::to_string(fused ? (ctx->plan.two_phase ? 2 : 1) + 2 * (n_classes - (int)idx.size())
+                                         : 2 * n_classes);
+    if (fused) j += ", \"grid\": " + std::to_string(ctx->plan.grid) + ", \"items\": " + std::to_string(ctx->plan.n_items);
+    j += ", \"candidates\": [";
+    for (int k = 0; k < kAllCandidates; ++k) j += (k ? ", \"" : "\"") + candidate_name(k) + "\"";
+    j += "], \"candidate_ms_per_step\": [";
+    for (int k = 0; k < kAllCandidates; ++k) {
+        std::snprintf(buf, sizeof buf, "%s%.4f", k ? ", " : "", tms[k]);
+        j += buf;
+    }
+    ctx->plan_desc = j + "]}";
     return BEC_OK;
 }
 

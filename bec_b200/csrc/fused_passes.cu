@@ -15,8 +15,8 @@ using stepk::PencilArgs;
 using stepk::VBlock;
 
 // ---------------------------------------------------------------- plane pass, N = 8, 16
-template <int N>
-__global__ void __launch_bounds__(128, 4) k_plane(float4 *__restrict__ state, int nz, int cells,
+template <int N, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_plane(float4 *__restrict__ state, int nz, int cells,
                                                const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
                                                const int *__restrict__ tlocal, const uint32_t *__restrict__ stepp)
 {
@@ -88,7 +88,7 @@ void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, co
     g_launches++;
 }
 
-template <int N>
+template <int N, int MINB>
 void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
                   const uint32_t *step, cudaStream_t s)
 {
@@ -97,10 +97,10 @@ void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, con
     const size_t smem = sizeof(float4) * 4 * W * N * N;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_plane<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_plane<N><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
+    k_plane<N, MINB><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
     g_launches++;
 }
 
@@ -127,13 +127,24 @@ bool fp32_fast_pencil_supported(const ClassGeom &c)
 }
 
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     const uint32_t *step, cudaStream_t s)
+                     const uint32_t *step, int occupancy, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
+    // occupancy 0: 16 warps per SM (8x8 / 16x16: 4 CTAs of 128 threads; 32x32: 8 CTAs of 64), no register spill;
+    // occupancy 1: 20 warps per SM (5 and 10 CTAs), 96 registers with a small spill
     switch (c.nx) {
-    case 8: launch_plane<8>(state, c, gp, tgroup, tlocal, step, s); break;
-    case 16: launch_plane<16>(state, c, gp, tgroup, tlocal, step, s); break;
-    case 32: launch_plane32s<8>(state, c, gp, tgroup, tlocal, step, s); break;
+    case 8:
+        if (occupancy) launch_plane<8, 5>(state, c, gp, tgroup, tlocal, step, s);
+        else launch_plane<8, 4>(state, c, gp, tgroup, tlocal, step, s);
+        break;
+    case 16:
+        if (occupancy) launch_plane<16, 5>(state, c, gp, tgroup, tlocal, step, s);
+        else launch_plane<16, 4>(state, c, gp, tgroup, tlocal, step, s);
+        break;
+    case 32:
+        if (occupancy) launch_plane32s<10>(state, c, gp, tgroup, tlocal, step, s);
+        else launch_plane32s<8>(state, c, gp, tgroup, tlocal, step, s);
+        break;
     default: break;
     }
 }

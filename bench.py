@@ -361,7 +361,7 @@ def main():
             kernels.append(dict(kernel=f"{kind}_{nx}x{ny}x{nz}", ms=t, bytes=bytes_launch,
                                 cells=nx * ny * nz * c["traj"]))
     per_pass = {k["kernel"]: {"ms": k["ms"], "frac": k["bytes"] / (k["ms"] * 1e-3) / 1e9 / peak} for k in kernels}
-    if plan.get("candidate", -1) >= 0:
+    if plan.get("fused_classes", 0) > 0:
         # the fused step kernel: one launch per step covering every register-path class
         fused_ms, fused_cells = eng.profile_fused_step(5)
         dom = dict(kernel="k_step", ms=fused_ms, bytes=32.0 * fused_cells, cells=fused_cells,

@@ -356,16 +356,18 @@ bec_status bec_checkpoint_load(bec_ctx *ctx, const void *buf, int64_t bytes);
 int32_t bec_step_graphs(const bec_ctx *ctx);
 
 /* Batched path: the schedule of a split step, written to out as a JSON object (len bytes at most,
- * NUL included). Grid classes whose planes are 8x8, 16x16 or 32x32 and whose nvz is 64, 128 or 256
- * run each step as ONE launch of a persistent kernel walking a work list of pencil-pass and
- * plane-pass items (a trajectory's plane items wait on its pencil items); the others launch two
- * passes each. Before the context's first step an autotuner times the work-list candidates (two
- * launches in two phases, or one launch interleaving each trajectory's plane items 0.5 to 4 waves
- * of the grid after its pencil items) on a copy of the state and keeps the fastest for this class
- * mix and device (cached per process). BEC_STEP_PLAN=unfused or =0..4 in the environment forces a
- * schedule, BEC_AUTOTUNE=0 takes the one-wave interleave untimed; every schedule computes the same
- * bits. The reference has one fixed schedule of eight launches per ensemble and step
- * (wigner.cu:178-199) with cuFFT plans built by batchfftPlan3d (batchfft.cu:22-100). */
+ * NUL included). Every grid class can run a step as two launches (its pencil and plane passes);
+ * the classes whose planes are 8x8, 16x16 or 32x32 and whose nvz is 64, 128 or 256 can instead
+ * run it together as ONE launch of a persistent kernel walking a work list of pencil-pass and
+ * plane-pass items (a trajectory's plane items wait on its pencil items). Before the context's
+ * first step an autotuner times the candidates on a copy of the state -- per-pass launches with
+ * the plane passes at 16 or at 20 warps per SM, and the work list run in two phases or
+ * interleaving each trajectory's plane items 0.5 to 4 waves of the grid after its pencil items --
+ * and keeps the fastest for this class mix and device (cached per process). BEC_STEP_PLAN in the
+ * environment forces one (unfused, unfused-20, or 0..4 for the work lists), BEC_AUTOTUNE=0 takes
+ * the per-pass launches untimed; every schedule computes the same bits. The reference has one fixed
+ * schedule of eight launches per ensemble and step (wigner.cu:178-199) with cuFFT plans built by
+ * batchfftPlan3d (batchfft.cu:22-100). */
 bec_status bec_step_plan(bec_ctx *ctx, char *out, int32_t len);
 
 /* Runs n_steps steady real-time steps (they advance the run like bec_evolve) with CUDA events on

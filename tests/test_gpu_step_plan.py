@@ -50,15 +50,17 @@ def _run(monkeypatch, plan, gss, groups=GROUPS):
 
 def test_every_schedule_gives_the_same_bits(monkeypatch, ground_states):
     ref = _run(monkeypatch, "unfused", ground_states)
-    assert ref["plan"]["plan"] == "unfused"
-    for plan in ["0", "1", "2", "3", "4", None]:
+    assert ref["plan"]["candidate"] == 0 and ref["plan"]["fused_classes"] == 0
+    for plan in ["unfused-20", "0", "1", "2", "3", "4", None]:
         got = _run(monkeypatch, plan, ground_states)
         p = got["plan"]
         if plan is None:
-            assert p["chosen"] in ("autotuned", "cached") and -1 <= p["candidate"] < 5
+            assert p["chosen"] in ("autotuned", "cached") and 0 <= p["candidate"] < 7
+        elif plan == "unfused-20":
+            assert p["chosen"] == "forced" and p["candidate"] == 1
         else:
-            assert p["chosen"] == "forced" and p["candidate"] == int(plan)
-        assert p["fused_classes"] == (4 if p["candidate"] >= 0 else 0)   # every class but the 2D slice
+            assert p["chosen"] == "forced" and p["candidate"] == int(plan) + 2
+        assert p["fused_classes"] == (4 if p["candidate"] >= 2 else 0)    # every class but the 2D slice
         np.testing.assert_array_equal(got["mom"], ref["mom"])
         np.testing.assert_array_equal(got["now"], ref["now"])
         for a, b in zip(got["states"], ref["states"]):
@@ -80,10 +82,11 @@ def test_autotuner_reports_timings(monkeypatch, ground_states):
     eng, _ = _three_classes(ground_states)
     p = eng.step_plan
     assert p["chosen"] in ("autotuned", "cached")
+    assert len(p["candidates"]) == 7
     if p["chosen"] == "autotuned":
-        ms = p["candidate_ms_per_step"]           # per-pass launches, then the fused candidates 0..4
-        assert len(ms) == 6 and all(v > 0 for v in ms)
-        assert ms[p["candidate"] + 1] == min(ms)
+        ms = p["candidate_ms_per_step"]           # per-pass launches at 16 and 20 warps per SM, the work lists 0..4
+        assert len(ms) == 7 and all(v > 0 for v in ms)
+        assert ms[p["candidate"]] == min(ms)
 
 
 def test_fused_plan_is_one_launch_per_step(monkeypatch, ground_states):
