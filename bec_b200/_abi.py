@@ -24,6 +24,7 @@ STATUS_NAMES = {
 # host element types of bec_init_groups
 BEC_HOST_C128 = 0
 BEC_HOST_C64 = 1
+BEC_HOST_R32 = 2
 
 BEC_PATH_FP64_PLAIN = 0
 BEC_PATH_FP32_BATCHED = 1

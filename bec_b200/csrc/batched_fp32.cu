@@ -71,9 +71,14 @@ __global__ void k_init(float4 *state, int cells, int ne, GroupParamsF gp, const 
     }
 }
 
+// ground-state value i of a complex128 (double2), complex64 (float2) or real FP32 (float) array, as float2
+__device__ __forceinline__ float2 gs_value(const double2 *p, int i) { return make_float2((float)p[i].x, (float)p[i].y); }
+__device__ __forceinline__ float2 gs_value(const float2 *p, int i) { return p[i]; }
+__device__ __forceinline__ float2 gs_value(const float *p, int i) { return make_float2(p[i], 0.f); }
+
 // The same initial state as k_init for a run of trajectories of one grid class that may belong to many
 // ensembles: trajectory t of the run takes its ensemble's parameters gp[tgroup[t]], its ground state
-// gs_ptrs[tgroup[t]] (complex128 or, with T = float2, complex64), and its Philox stream tlocal[t].
+// gs_ptrs[tgroup[t]] (complex128, complex64 or real FP32 values, by T), and its Philox stream tlocal[t].
 template <typename T>
 __global__ void k_init_batched(float4 *state, int cells, int n_traj, const int *__restrict__ tgroup,
                                const int *__restrict__ tlocal, const GroupParamsF *__restrict__ gp,
@@ -90,9 +95,8 @@ __global__ void k_init_batched(float4 *state, int cells, int n_traj, const int *
         normals4<float>(seed, (uint32_t)tlocal[t], 0u, (uint32_t)i, RNG_TAG_INIT, r);
         const float2 ea = make_float2(0.5f * r[0], 0.5f * r[1]);
         const float2 eb = make_float2(0.5f * r[2], 0.5f * r[3]);
-        const T g = static_cast<const T *>(gs_ptrs[grp])[i];
-        state[idx] = make_float4((float)g.x + P.init_a * ea.x, (float)g.y + P.init_a * ea.y,
-                                 P.init_b * eb.x, P.init_b * eb.y);
+        const float2 g = gs_value(static_cast<const T *>(gs_ptrs[grp]), i);
+        state[idx] = make_float4(g.x + P.init_a * ea.x, g.y + P.init_a * ea.y, P.init_b * eb.x, P.init_b * eb.y);
     }
 }
 
@@ -407,13 +411,17 @@ void fp32_init_group(float4 *state, int cells, int ne, const GroupParamsF &gp, c
 }
 
 void fp32_init_batched(float4 *state, int cells, int n_traj, const int *tgroup, const int *tlocal,
-                       const GroupParamsF *gp, const void *const *gs_ptrs, bool c64, cudaStream_t s)
+                       const GroupParamsF *gp, const void *const *gs_ptrs, int host_type, cudaStream_t s)
 {
     size_t n = (size_t)cells * n_traj;
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 32) blocks = 148 * 32;
-    if (c64) k_init_batched<float2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
-    else k_init_batched<double2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
+    if (host_type == BEC_HOST_R32)
+        k_init_batched<float><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
+    else if (host_type == BEC_HOST_C64)
+        k_init_batched<float2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
+    else
+        k_init_batched<double2><<<blocks, 256, 0, s>>>(state, cells, n_traj, tgroup, tlocal, gp, gs_ptrs);
     g_launches++;
 }
 

@@ -1780,7 +1780,8 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
                            int32_t host_type)
 {
     if (!ctx) return BEC_ERR_INVALID_ARG;
-    if (n < 0 || (n > 0 && (!groups || !psi_gs)) || (host_type != BEC_HOST_C128 && host_type != BEC_HOST_C64))
+    if (n < 0 || (n > 0 && (!groups || !psi_gs)) ||
+        (host_type != BEC_HOST_C128 && host_type != BEC_HOST_C64 && host_type != BEC_HOST_R32))
         return fail(ctx, BEC_ERR_INVALID_ARG, "bad bec_init_groups arguments");
     const int ng = (int)ctx->groups.size();
     std::vector<char> listed(ng, 0);
@@ -1795,10 +1796,14 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
     if (ctx->path == BEC_PATH_FP64_PLAIN) {
         const long long l0 = g_launches;
         for (int i = 0; i < n; ++i) {
-            if (c64) {
+            if (c64 || host_type == BEC_HOST_R32) {
                 const int cells = ctx->groups[groups[i]].gd.cells;
                 const float *f = static_cast<const float *>(psi_gs[i]);
-                std::vector<double> d(f, f + 2 * (size_t)cells);
+                std::vector<double> d(2 * (size_t)cells, 0.0);
+                for (size_t k = 0; k < (size_t)cells; ++k) {
+                    if (c64) { d[2 * k] = f[2 * k]; d[2 * k + 1] = f[2 * k + 1]; }
+                    else d[2 * k] = f[k];
+                }
                 if ((st = bec_init_group(ctx, groups[i], d.data(), nullptr))) return st;
             } else if ((st = bec_init_group(ctx, groups[i], static_cast<const double *>(psi_gs[i]), nullptr))) {
                 return st;
@@ -1813,7 +1818,7 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
     if (!ctx->d_gs_ptrs) CKC(dalloc(ctx, &ctx->d_gs_ptrs, (size_t)ng));
     // the staging area holds the listed ground states in group order at the call's element size, so that
     // consecutive groups whose host buffers are adjacent arrive in one copy
-    const size_t esz = c64 ? sizeof(float2) : sizeof(double2);
+    const size_t esz = host_type == BEC_HOST_R32 ? sizeof(float) : c64 ? sizeof(float2) : sizeof(double2);
     std::vector<size_t> off(ng + 1, 0);
     for (int g = 0; g < ng; ++g) off[g + 1] = off[g] + esz * (size_t)ctx->groups[g].gd.cells;
     if ((st = gs_stage_ready(ctx))) return st;
@@ -1850,7 +1855,7 @@ bec_status bec_init_groups(bec_ctx *ctx, int32_t n, const int32_t *groups, const
         for (const auto &r : runs) {
             float4 *base = c.state + (size_t)r.first * c.geom.cells;
             fp32_init_batched(base, c.geom.cells, r.second, c.d_tgroup + r.first, c.d_tlocal + r.first, ctx->d_gparams,
-                              ctx->d_gs_ptrs, c64, s);
+                              ctx->d_gs_ptrs, host_type, s);
             CKL();
             ClassGeom sub = c.geom;
             sub.n_traj = r.second;

@@ -101,9 +101,9 @@ struct ZPassArgs {
 void fp32_init_group(float4 *state, int cells, int ne, const GroupParamsF &gp, const double2 *gs,
                      const float2 *noise, cudaStream_t s);
 // k_init for n_traj consecutive trajectories of a class from many ensembles: tgroup / tlocal of the run,
-// gs_ptrs[group] the ensemble's device ground state, complex64 when c64, else complex128
+// gs_ptrs[group] the ensemble's device ground state, in the element type of host_type (BEC_HOST_*)
 void fp32_init_batched(float4 *state, int cells, int n_traj, const int *tgroup, const int *tlocal,
-                       const GroupParamsF *gp, const void *const *gs_ptrs, bool c64, cudaStream_t s);
+                       const GroupParamsF *gp, const void *const *gs_ptrs, int host_type, cudaStream_t s);
 // x-space -> stored representation (inverse transform over x and y)
 void fp32_prep(float4 *state, const ClassGeom &c, const float2 *tw_x, const float2 *tw_y, cudaStream_t s);
 // stored representation -> x-space (forward transform over x and y)

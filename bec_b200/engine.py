@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from ._abi import (BecDerived, BecGsOpts, BecGsReport, BecMoments, BecObs, BecParams, BecSchedule,
-                   BEC_GS_FIXED_STEPS, BEC_HOST_C128, BEC_HOST_C64, BEC_LR_CONSTANT, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
+                   BEC_GS_FIXED_STEPS, BEC_HOST_C128, BEC_HOST_C64, BEC_HOST_R32, BEC_LR_CONSTANT, BEC_PATH_FP32_BATCHED, BEC_PATH_FP64_PLAIN, STATUS_NAMES)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbec.so")
@@ -246,12 +246,14 @@ class Engine:
         """bec_init_groups: initialise many groups in one call (vacuum noise from Philox).
 
         psi_gs[i] is the ground state of groups[i]; complex64 arrays are passed as complex64
-        (half the host-to-device bytes), anything else as complex128. Pinned arrays copy fastest."""
+        (half the host-to-device bytes), float32 arrays as real FP32 ground states (a quarter),
+        anything else as complex128. Pinned arrays copy fastest."""
         groups = [int(g) for g in groups]
         if len(groups) != len(psi_gs):
             raise ValueError("one ground state per group")
         c64 = len(psi_gs) > 0 and all(np.asarray(a).dtype == np.complex64 for a in psi_gs)
-        dt = np.complex64 if c64 else np.complex128
+        r32 = len(psi_gs) > 0 and all(np.asarray(a).dtype == np.float32 for a in psi_gs)
+        dt = np.complex64 if c64 else np.float32 if r32 else np.complex128
         arrs = []
         for g, a in zip(groups, psi_gs):
             a = np.ascontiguousarray(a, dtype=dt).reshape(-1)
@@ -263,7 +265,8 @@ class Engine:
         n = len(groups)
         gi = (C.c_int32 * max(n, 1))(*groups)
         ptrs = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrs])
-        self._check(lib().bec_init_groups(self._h, n, gi, ptrs, BEC_HOST_C64 if c64 else BEC_HOST_C128),
+        self._check(lib().bec_init_groups(self._h, n, gi, ptrs,
+                                          BEC_HOST_C64 if c64 else BEC_HOST_R32 if r32 else BEC_HOST_C128),
                     "bec_init_groups")
 
     def start_evolution(self):

@@ -39,6 +39,7 @@ N_TRAJ = 1024
 # stopping rules of the ground-state leg: |d mu|/mu between checks below 1e-7 stops every held-out set
 # within 1e-6 of its converged mu (measured); 1e-6 is the reference-style test on the change alone
 GS_TOL, GS_REF_TOL = 1e-7, 1e-6
+GS_TRAIN_STEPS = 30000
 WORKLOAD = "uneven-ensembles-1024"
 
 
@@ -225,7 +226,9 @@ def gs_warmstart_leg(n_train, n_eval, tol, ref_tol):
     t0 = time.time()
     tr = W.sample_params(n_train, 3)
     ev = W.sample_params(n_eval, 4)
-    kw = dict(tol=1e-6, check_every=20)
+    # training ground states converged at the same accurate rule as the evaluation: the network learns
+    # coefficients good to ~1e-3, not the ~2e-3 of states stopped at |d mu|/mu < 1e-6
+    kw = dict(tol=tol, check_every=20, max_steps=40000)
     n_pod = min(512, n_train)
     first = W.ground_states(tr[:n_pod], want_profiles=True, **kw)
     basis, _ = W.pod_basis(first["profiles"])
@@ -236,7 +239,7 @@ def gs_warmstart_leg(n_train, n_eval, tol, ref_tol):
         c_tr = np.concatenate([c_tr, rest["coef"]])
         gen_s += rest["seconds"]
     t_train = time.time()
-    ws, hist = W.train(tr, c_tr, steps=12000)
+    ws, hist = W.train(tr, c_tr, steps=GS_TRAIN_STEPS)
     t_train = time.time() - t_train
     ref = W.ground_states(ev, basis=basis, tol=1e-10, res_tol=1e-9, check_every=20, max_steps=40000)
     mu_star = ref["mu"]
@@ -269,7 +272,8 @@ def gs_warmstart_leg(n_train, n_eval, tol, ref_tol):
                    f"({float(ref['steps'].mean()):.0f} steps mean); the FP32 fixed point lies 3e-7 to 4e-7 from "
                    "the FP64 one",
         "inference_s": t_inf,
-        "training": {"ground_states_device_s": gen_s, "train_s": t_train, "loss_last": float(hist[-10:].mean())},
+        "training": {"ground_states_device_s": gen_s, "rule": f"|d mu|/mu < {tol:g}, residual < {10 * tol:g}",
+                     "adam_steps": GS_TRAIN_STEPS, "train_s": t_train, "loss_last": float(hist[-10:].mean())},
         "wall_s": time.time() - t0,
     }
 
@@ -382,14 +386,14 @@ def main():
                  "frac": (step_gbs / ws if ws > 1 else step_gbs) / peak,
                  "note": "32 B/cell/step algorithmic bytes of the whole step, all kernels"}
 
-    # e2e through the C ABI: host ground states (pinned, complex64: the FP32 path rounds them to FP32 on
-    # the device either way) -> one batched init of every ensemble -> pi/2 -> K steps -> moments to host
-    # one pinned buffer, the groups' ground states back to back in group order (bec_init_groups then
-    # copies them in one transfer)
-    pin = torch.empty(2 * sum(a.size for a in host_gs), dtype=torch.float32, pin_memory=True).numpy().view(np.complex64)
+    # e2e through the C ABI: host ground states (pinned, real FP32: the ground states are real, and the FP32
+    # path rounds them to FP32 on the device either way) -> one batched init of every ensemble -> pi/2 ->
+    # K steps -> moments to host; one pinned buffer, the groups' ground states back to back in group order
+    # (bec_init_groups then copies them in one transfer)
+    pin = torch.empty(sum(a.size for a in host_gs), dtype=torch.float32, pin_memory=True).numpy()
     host_gs64, o = [], 0
     for a in host_gs:
-        pin[o:o + a.size] = a
+        pin[o:o + a.size] = a.real
         host_gs64.append(pin[o:o + a.size])
         o += a.size
     torch.cuda.synchronize()
@@ -406,11 +410,11 @@ def main():
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = 8.0 * total_cells / args.steps
+    h2d = 4.0 * total_cells / args.steps
     d2h = 40.0 * mom.shape[0] * mom.shape[1] / args.steps
     e2e = {"value": n_traj_total * args.steps / e2e_s, "unit": "traj-steps/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "note": "batched init from pinned complex64 host ground states + pi/2 + K steps + moments to host, per call"}
+           "note": "batched init from pinned real FP32 host ground states + pi/2 + K steps + moments to host, per call"}
 
     # ensemble observables of the global batch: one small FP64 all-reduce of the per-sample moments
     mom_all = D.allreduce_moments(mom, mine, len(all_groups), device="cuda")

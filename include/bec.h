@@ -242,14 +242,17 @@ bec_status bec_warmstart_set_basis(bec_ctx *ctx, int32_t nvx, int32_t nvy, int32
  * noise have been copied to the device (the caller may reuse them); the kernels run on. */
 bec_status bec_init_group(bec_ctx *ctx, int32_t group, const double *psi_gs, const double *noise);
 
-/* Host element types of bec_init_groups' ground states */
-enum { BEC_HOST_C128 = 0, BEC_HOST_C64 = 1 };
+/* Host element types of bec_init_groups' ground states. BEC_HOST_R32 is real FP32 (imaginary part
+ * zero): an imaginary-time ground state from Thomas-Fermi is real, every factor the loop applies
+ * being real, so a quarter of the complex128 bytes carries it exactly to the FP32 path. */
+enum { BEC_HOST_C128 = 0, BEC_HOST_C64 = 1, BEC_HOST_R32 = 2 };
 
 /* bec_init_group (noise == NULL) for n distinct groups at once: the same initial states bit for
- * bit. psi_gs[i] is the x-space ground state of groups[i]. It holds cells interleaved complex
- * values, complex128 (BEC_HOST_C128) or complex64 (BEC_HOST_C64). The batched FP32 path rounds a
- * ground state to FP32 on the device either way, so complex64 halves the host-to-device copy
- * without changing any result. The batched path copies the ground states (consecutive groups whose host
+ * bit. psi_gs[i] is the x-space ground state of groups[i]. It holds cells values, interleaved
+ * complex128 (BEC_HOST_C128) or complex64 (BEC_HOST_C64), or real FP32 (BEC_HOST_R32). The batched
+ * FP32 path rounds a ground state to FP32 on the device either way, so complex64 halves the
+ * host-to-device copy, and real FP32 halves it again for a real ground state, without changing
+ * any result. The batched path copies the ground states (consecutive groups whose host
  * arrays lie back to back in memory in one transfer), then launches one
  * initialisation kernel and one preparation pass per run of consecutive trajectories of a grid
  * class, not one pair per group. The plain path initialises group by group. BEC_ERR_INVALID_ARG

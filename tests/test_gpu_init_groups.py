@@ -4,7 +4,8 @@ The batched call must give the same initial states, bit for bit, as bec_init_gro
 once per group: the same per-cell arithmetic runs in one kernel and one preparation pass per
 run of consecutive trajectories instead of one pair per group. A complex64 ground state that
 is the complex128 one rounded to FP32 gives the same states too, because the FP32 path
-rounds the ground state to FP32 on the device either way.
+rounds the ground state to FP32 on the device either way; so does a real FP32 ground state
+(BEC_HOST_R32) of a real profile.
 """
 import numpy as np
 import pytest
@@ -69,6 +70,9 @@ def test_batched_init_bit_identical():
     # ground states back to back in one host buffer: consecutive groups arrive in one copy
     assert_same(ref, run(lambda eng, gs: eng.init_groups(range(len(gs)), contiguous_views(gs, np.complex64))))
     assert_same(ref, run(lambda eng, gs: eng.init_groups(range(len(gs)), contiguous_views(gs, np.complex128))))
+    # real FP32 ground states (BEC_HOST_R32): the Thomas-Fermi profiles are real, so the same states
+    assert_same(ref, run(lambda eng, gs: eng.init_groups(range(len(gs)), contiguous_views(
+        [a.real for a in gs], np.float32))))
 
 
 def contiguous_views(arrays, dtype):
@@ -99,6 +103,12 @@ def test_batched_init_plain_path():
     ref = run(per_group, path=BEC_PATH_FP64_PLAIN, groups=groups, steps=2)
     got = run(lambda eng, gs: eng.init_groups([0, 1], gs), path=BEC_PATH_FP64_PLAIN, groups=groups, steps=2)
     assert_same(ref, got)
+    # real FP32 ground states reach the FP64 path as their FP32 values
+    r32 = run(lambda eng, gs: eng.init_groups([0, 1], [a.real.astype(np.float32) for a in gs]),
+              path=BEC_PATH_FP64_PLAIN, groups=groups, steps=2)
+    r64 = run(lambda eng, gs: eng.init_groups([0, 1], [a.real.astype(np.float32).astype(np.complex128) for a in gs]),
+              path=BEC_PATH_FP64_PLAIN, groups=groups, steps=2)
+    assert_same(r64, r32)
 
 
 def test_batched_init_rejects_bad_arguments():

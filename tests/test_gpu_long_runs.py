@@ -117,59 +117,66 @@ def test_ensemble_16x16x128_200ms():
     assert err["axial_ratio"] < 3e-2
 
 
-def _traj_obs(tm, d):
-    """per-trajectory N1, N2, visibility and phase from per-trajectory moments [ne, 5]"""
-    n1 = np.array([OBS.populations(r, d, 1)[0] for r in tm])
-    n2 = np.array([OBS.populations(r, d, 1)[1] for r in tm])
-    vis = np.array([OBS.visibility(r, d, 1) for r in tm])
-    ph = np.arctan2(tm[:, 4], tm[:, 3])
-    return n1, n2, vis, ph
+def _ensemble_obs(mom, traj, axial, d, ne):
+    """Per-sample ensemble observables of a run: N1, N2, visibility, phase, phase noise (circular spread of the
+    per-trajectory phases), and per axial sample the ratio (a - b)/(a + b)(z)."""
+    n1, n2 = OBS.populations(mom.T, d, ne)
+    vis = np.array([OBS.visibility(m, d, ne) for m in mom])
+    phase = np.array([OBS.phase(m) for m in mom])
+    noise = np.array([_phase_spread(t) for t in traj])
+    ratio = np.array([OBS.axial_ratio(a, d, ne) for a in axial])
+    return dict(N1=n1, N2=n2, visibility=vis, phase=phase, phase_noise=noise, axial_ratio=ratio)
+
+
+def _deviation(x, y, name):
+    """max over samples of |x - y| (phases compared on the circle)"""
+    if name == "phase":
+        return float(np.max(np.abs(np.angle(np.exp(1j * (x - y))))))
+    return float(np.max(np.abs(x - y)))
 
 
 def test_spin_echo_32x32x256_one_second():
-    """Over the full second the trajectories of the two runs part (the dynamics amplify FP32 rounding
-    differences exponentially at N = 70000; see the design notes for the FP64 oracle's own sensitivity),
-    so each trajectory is compared over the first 1000 steps and the ensemble observables over the whole
-    run against their statistical error: 4 x the standard error of a 4-trajectory mean, from the spread
-    of the trajectories of both runs."""
+    """The trajectories of the FP32 run part from the FP64 oracle's within ~1500 steps: at N = 70000 the
+    dynamics amplify any rounding-size difference about a hundredfold per 500 steps, which the oracle
+    shows on itself (its run with the stored state rounded to FP32 after every step, the second fixture,
+    parts from the unrounded one the same way). So each trajectory is compared over the first 1000 steps,
+    and each ensemble observable over the whole second against the FP64 oracle's own deviation under
+    FP32 rounding: the FP32 run may differ from the oracle by at most 3 x as much as the rounded oracle run
+    does (plus a floor of 1e-3 of the observable's scale)."""
     meta, fx = _load("spin_echo_32x32x256_4traj.npz")
+    _, fr = _load("spin_echo_32x32x256_4traj_fp32round.npz")
     p = spin_echo_32x32x256(ne=4, seed=4)
     eng, rep, mom, traj, axial = _engine_run(p, meta)
     assert rep.mu == pytest.approx(float(fx["gs_mu"]), rel=1e-10)
-    err = _compare("long_spin_echo_32x32x256", p, meta, fx, eng, mom, traj, axial)
+    _compare("long_spin_echo_32x32x256", p, meta, fx, eng, mom, traj, axial)
     d = eng.derived[0]
-    to = fx["traj_moments"]
     ne = p.ne
     # per trajectory, early: samples after 500 and 1000 steps
+    to = fx["traj_moments"]
     early = np.abs(traj[:2, :, 1:3] - to[:2, :, 1:3]) / to[:2, :, 1:3]
-    record("long_spin_echo_early", traj_population_1000=float(early.max()))
     assert early.max() < 2e-4
-    # ensemble observables against their statistical error
-    worst = {}
-    for k in range(len(mom)):
-        oe, oo = _traj_obs(traj[k], d), _traj_obs(to[k], d)
-        ens_e = (*OBS.populations(mom[k], d, ne), OBS.visibility(mom[k], d, ne), OBS.phase(mom[k]))
-        ens_o = (*OBS.populations(fx["moments"][k], d, ne), OBS.visibility(fx["moments"][k], d, ne),
-                 OBS.phase(fx["moments"][k]))
-        for name, i in (("N1", 0), ("N2", 1), ("visibility", 2), ("phase", 3)):
-            if name == "phase":
-                diff = abs(np.angle(np.exp(1j * (ens_e[i] - ens_o[i]))))
-                spread = [np.sqrt(max(-2 * np.log(max(abs(np.exp(1j * o[i]).mean()), 1e-300)), 0.0)) for o in (oe, oo)]
-            else:
-                diff = abs(ens_e[i] - ens_o[i])
-                spread = [o[i].std(ddof=1) for o in (oe, oo)]
-            sigma = np.sqrt(spread[0] ** 2 + spread[1] ** 2) / np.sqrt(ne)
-            worst[name] = max(worst.get(name, 0.0), diff / max(sigma, 1e-12))
-    record("long_spin_echo_sigmas", **worst)
-    for name, z in worst.items():
-        assert z < 4.0, (name, z)
+    # ensemble observables against the oracle's deviation under FP32 rounding
+    e = _ensemble_obs(mom, traj, axial, d, ne)
+    o = _ensemble_obs(fx["moments"], fx["traj_moments"], fx["axial"], d, ne)
+    r = _ensemble_obs(fr["moments"], fr["traj_moments"], fr["axial"], d, ne)
+    scale = dict(N1=o["N1"].max(), N2=o["N1"].max(), visibility=1.0, phase=np.pi, phase_noise=np.pi, axial_ratio=1.0)
+    sub = ne * d.nvx * d.nvy * d.V / 2.0
+    keep = [np.abs(a[:, 0] + a[:, 1] - 2 * sub) > 0.2 * np.abs(a[:, 0] + a[:, 1] - 2 * sub).max() for a in fx["axial"]]
+    out = {"early_traj_population": float(early.max())}
+    for name in ("N1", "N2", "visibility", "phase", "phase_noise", "axial_ratio"):
+        if name == "axial_ratio":
+            dev_e = max(float(np.abs(x - y)[k].max()) for x, y, k in zip(e[name], o[name], keep))
+            dev_r = max(float(np.abs(x - y)[k].max()) for x, y, k in zip(r[name], o[name], keep))
+        else:
+            dev_e, dev_r = _deviation(e[name], o[name], name), _deviation(r[name], o[name], name)
+        out[name] = dev_e
+        out[name + "_rounded_oracle"] = dev_r
+        assert dev_e <= 3.0 * dev_r + 1e-3 * scale[name], (name, dev_e, dev_r)
     # final pi/2 at 50 phase points: closed form from the FP32 run's moments against the oracle's literal
-    # rotation of its own state, relative to the spread of the trajectories' rotated populations
+    # rotation of its own state, against the same for the rounded oracle run
     scan = eng.phase_scan(0, mom[-1], fx["alpha"]) * ne
-    rot = fx["rotated_sums"]
-    per_traj = np.array([[OBS.rotated(r, d, 1, a) for a in fx["alpha"]] for r in to[-1]])   # [ne, 50, 2]
-    sigma_scan = per_traj.std(axis=0, ddof=1) * np.sqrt(ne) * np.sqrt(2.0)
-    z_scan = float(np.max(np.abs(scan - rot) / sigma_scan))
-    record("long_spin_echo_phase_scan", phase_scan=float(np.max(np.abs(scan - rot)) / np.abs(rot).max()),
-           phase_scan_sigmas=z_scan)
-    assert z_scan < 4.0
+    dev_scan = float(np.max(np.abs(scan - fx["rotated_sums"])) / np.abs(fx["rotated_sums"]).max())
+    dev_scan_r = float(np.max(np.abs(fr["rotated_sums"] - fx["rotated_sums"])) / np.abs(fx["rotated_sums"]).max())
+    out["phase_scan"], out["phase_scan_rounded_oracle"] = dev_scan, dev_scan_r
+    record("long_spin_echo_vs_rounded_oracle", **out)
+    assert dev_scan <= 3.0 * dev_scan_r + 1e-3

@@ -117,7 +117,7 @@ def test_installed_basis_projection_and_warm_start():
 
 @pytest.mark.gpu
 def test_warm_start_pipeline_beats_cold_start():
-    out = W.run(n_train=512, n_eval=32, n_pod=128, seed=5, train_steps=1500, grid=(16, 16, 128),
+    out = W.run(n_train=512, n_eval=32, n_pod=128, seed=5, train_steps=1500, tol=1e-6, grid=(16, 16, 128),
                 log=lambda *a: None)
     assert out["cold_converged"] == 1.0 and out["warm_converged"] == 1.0
     assert out["speedup_steps"] > 3.0
