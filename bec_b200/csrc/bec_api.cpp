@@ -62,6 +62,8 @@ struct ClassRec {
     int traj_offset = 0;      // global index of the class's first trajectory
     std::vector<int> groups;  // group indices in this class
     float2 *kin_tab[2] = {nullptr, nullptr};   // kinetic phase tables for kick fractions 0.5 and 1 (register pencils)
+    bool tma_pick = true;     // the TMA pencil schedules use the TMA kernel for this class (autotuned per class)
+    double pencil_ms[2] = {-1.0, -1.0};        // autotuner: register / TMA pencil pass, ms per launch
 };
 
 } // namespace
@@ -83,6 +85,8 @@ struct bec_ctx {
     std::vector<char> fused;             // per class: 1 when its passes run in the fused step
     int plan_mode = -2;                  // -2: not chosen yet, else the schedule candidate (ensure_plan)
     int plane_occupancy = 0;             // per-pass plane launches: 0 = 16 warps per SM, 1 = 20
+    bool pencil_tma = false;             // per-pass pencil launches: the persistent TMA kernel (pencil_tma.cu)
+    int *d_pflags = nullptr;             // batched: [0] error flag of the TMA pencil pass, [1] a flag nothing sets
     std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
     long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
@@ -395,8 +399,12 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
             if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
             const float frac = kf;
             const float2 *kin = frac == 1.0f ? c.kin_tab[1] : frac == 0.5f ? c.kin_tab[0] : nullptr;
-            fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, frac, z.scale * z.out_scale,
-                             mf, observe ? c.obs_partial : nullptr, z.out_scale, kin, ctx->stream);
+            if (!observe && ctx->pencil_tma && c.tma_pick && fp32_pencil_tma_supported(c.geom))
+                CKC(fp32_pencil_tma(c.state, c.geom, twf, frac, z.scale * z.out_scale, mf, kin, ctx->d_pflags,
+                                    ctx->d_pflags + 1, ctx->stream));
+            else
+                fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, frac, z.scale * z.out_scale,
+                                 mf, observe ? c.obs_partial : nullptr, z.out_scale, kin, ctx->stream);
             if (observe) c.obs_tiles = fp32_fast_pencil_tiles(c.geom);
         } else {
             float2 *tz;
@@ -469,18 +477,61 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
 // The split-step schedule of a batched context, chosen once before its first step. Candidates:
 //   0  per-pass launches, plane passes at 16 warps per SM (no register spill)
 //   1  per-pass launches, plane passes at 20 warps per SM (96 registers, a small spill)
-//   2 + k  the fused step kernel on work list k (two-phase, interleaved at 0.5, 1, 2, 4 waves)
-// BEC_STEP_PLAN in the environment forces one ("unfused" = 0, "unfused-20" = 1, "0".."4" = fused k);
-// otherwise a choice cached for the same class mix on this device is reused, or every candidate is timed
-// on a copy of the state (BEC_AUTOTUNE=0 skips the timing and takes candidate 0).
-constexpr int kPerPassCandidates = 2;
+//   2, 3  as 0, 1 with the non-observing pencil passes on the persistent TMA kernel
+//   4 + k  the fused step kernel on work list k (two-phase, interleaved at 0.5, 1, 2, 4 waves)
+// BEC_STEP_PLAN in the environment forces one ("unfused" = 0, "unfused-20" = 1, "unfused-tma" = 2,
+// "unfused-20-tma" = 3, "0".."4" = fused k); otherwise a choice cached for the same class mix on this
+// device is reused, or every candidate is timed on a copy of the state (BEC_AUTOTUNE=0 skips the timing
+// and takes candidate 0).
+constexpr int kPerPassCandidates = 4;
 constexpr int kAllCandidates = kPerPassCandidates + kStepCandidates;
+const char *const kPerPassNames[kPerPassCandidates] = {"unfused", "unfused-20", "unfused-tma", "unfused-20-tma"};
 
 std::string candidate_name(int c)
 {
-    if (c == 0) return "per-pass launches, 16 warps per SM";
-    if (c == 1) return "per-pass launches, 20 warps per SM";
+    if (c < kPerPassCandidates)
+        return std::string("per-pass launches, ") + (c & 1 ? "20" : "16") + " warps per SM" +
+               (c >= 2 ? ", TMA pencil pass" : "");
     return std::string("fused ") + step_plan_name(c - kPerPassCandidates);
+}
+
+bec_status check_step_error(bec_ctx *ctx);
+
+// Per grid class, the faster of the two pencil kernels for the full-kick pass of a steady step: the register
+// kernel (16 pencils per CTA, two CTAs per SM) or the persistent TMA kernel (three CTAs per SM, the next
+// tile's load in flight). Both compute the same bits; each is timed over three launches after one warm-up on
+// the current state (the caller restores it).
+bec_status pick_pencil_kernels(bec_ctx *ctx)
+{
+    for (auto &c : ctx->classes) {
+        c.tma_pick = true;
+        c.pencil_ms[0] = c.pencil_ms[1] = -1.0;
+        if (c.geom.n_traj == 0 || !ctx->use_fast || !fp32_fast_pencil_supported(c.geom) ||
+            !fp32_pencil_tma_supported(c.geom) || !c.kin_tab[1])
+            continue;
+        float2 *twf;
+        bec_status st;
+        if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
+        const float scale = (float)(1.0 / (double)c.geom.cells);
+        for (int kind = 0; kind < 2; ++kind) {
+            for (int r = 0; r < 4; ++r) {
+                if (r == 1) CKC(cudaEventRecord(ctx->ev0, ctx->stream));
+                if (kind == 0)
+                    fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, 1.0f, scale, nullptr, nullptr,
+                                     1.0f, c.kin_tab[1], ctx->stream);
+                else
+                    CKC(fp32_pencil_tma(c.state, c.geom, twf, 1.0f, scale, nullptr, c.kin_tab[1], ctx->d_pflags,
+                                        ctx->d_pflags + 1, ctx->stream));
+            }
+            CKC(cudaEventRecord(ctx->ev1, ctx->stream));
+            CKC(cudaEventSynchronize(ctx->ev1));
+            float ms = 0.f;
+            CKC(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            c.pencil_ms[kind] = ms / 3.0;
+        }
+        c.tma_pick = c.pencil_ms[1] < c.pencil_ms[0];
+    }
+    return BEC_OK;
 }
 
 bec_status ensure_plan(bec_ctx *ctx)
@@ -518,13 +569,15 @@ bec_status ensure_plan(bec_ctx *ctx)
     auto apply = [&](int c) -> bec_status {
         if (c < kPerPassCandidates) {
             ctx->plan.ready = false;
-            ctx->plane_occupancy = c;
+            ctx->plane_occupancy = c & 1;
+            ctx->pencil_tma = c >= 2;
             for (int ci : idx) ctx->fused[ci] = 0;
             return BEC_OK;
         }
         if (step_plan_build(ctx->plan, geoms, devs, offs, c - kPerPassCandidates, ctx->stream) != cudaSuccess)
             return fail(ctx, BEC_ERR_CUDA, "fused step plan");
         ctx->plane_occupancy = 0;
+        ctx->pencil_tma = false;
         for (int ci : idx) ctx->fused[ci] = 1;
         return BEC_OK;
     };
@@ -532,8 +585,9 @@ bec_status ensure_plan(bec_ctx *ctx)
     std::string how = "default";
     std::vector<double> tms(kAllCandidates, -1.0);
     bec_status st;
-    if (fs == "unfused" || fs == "unfused-20") {
-        cand = fs == "unfused" ? 0 : 1;
+    const int named = (int)(std::find(kPerPassNames, kPerPassNames + kPerPassCandidates, fs) - kPerPassNames);
+    if (named < kPerPassCandidates) {
+        cand = named;
         how = "forced";
     } else if (!fs.empty()) {
         const int k = std::atoi(fs.c_str());
@@ -542,6 +596,9 @@ bec_status ensure_plan(bec_ctx *ctx)
         cand = kPerPassCandidates + k;
         how = "forced";
     } else if (step_plan_cached(geoms, &cand)) {
+        // the candidate, and above bit 8 the per-class pencil kernel picks
+        for (size_t ci = 0; ci < ctx->classes.size() && ci < 23; ++ci) ctx->classes[ci].tma_pick = (cand >> (8 + ci)) & 1;
+        cand &= 0xFF;
         how = "cached";
     } else {
         const char *at = std::getenv("BEC_AUTOTUNE");
@@ -561,7 +618,7 @@ bec_status ensure_plan(bec_ctx *ctx)
                 }
                 const bool had_pulse = ctx->has_pulse;
                 ctx->has_pulse = false;
-                st = BEC_OK;
+                st = pick_pencil_kernels(ctx);
                 double best = 1e30;
                 for (int k = 0; k < n_cand && st == BEC_OK; ++k) {
                     if ((st = apply(k))) break;
@@ -590,11 +647,12 @@ bec_status ensure_plan(bec_ctx *ctx)
                 cudaFree(save);
                 ctx->has_pulse = had_pulse;
                 if (st) return st;
-                int err = 0;
-                CKC(step_read_error(ctx->plan, &err, ctx->stream));
-                if (err) return fail(ctx, BEC_ERR_CUDA, "fused step: a dependency wait gave up");
+                if ((st = check_step_error(ctx))) return st;
                 how = "autotuned";
-                step_plan_remember(geoms, cand);
+                int picks = 0;
+                for (size_t ci = 0; ci < ctx->classes.size() && ci < 23; ++ci)
+                    picks |= (ctx->classes[ci].tma_pick ? 1 : 0) << (8 + ci);
+                step_plan_remember(geoms, cand | picks);
             } else {
                 cudaGetLastError();
             }
@@ -613,7 +671,18 @@ bec_status ensure_plan(bec_ctx *ctx)
                     std::to_string(fused ? (ctx->plan.two_phase ? 2 : 1) + 2 * (n_classes - (int)idx.size())
                                          : 2 * n_classes);
     if (fused) j += ", \"grid\": " + std::to_string(ctx->plan.grid) + ", \"items\": " + std::to_string(ctx->plan.n_items);
-    j += ", \"candidates\": [";
+    j += ", \"pencil_kernels\": [";
+    bool firstc = true;
+    for (auto &c : ctx->classes) {
+        if (c.geom.n_traj == 0) continue;
+        std::snprintf(buf, sizeof buf, "%s{\"grid\": [%d, %d, %d], \"tma\": %s, \"register_ms\": %.4f, \"tma_ms\": %.4f}",
+                      firstc ? "" : ", ", c.geom.nx, c.geom.ny, c.geom.nz,
+                      ctx->pencil_tma && c.tma_pick && fp32_pencil_tma_supported(c.geom) ? "true" : "false",
+                      c.pencil_ms[0], c.pencil_ms[1]);
+        j += buf;
+        firstc = false;
+    }
+    j += "], \"candidates\": [";
     for (int k = 0; k < kAllCandidates; ++k) j += (k ? ", \"" : "\"") + candidate_name(k) + "\"";
     j += "], \"candidate_ms_per_step\": [";
     for (int k = 0; k < kAllCandidates; ++k) {
@@ -678,6 +747,14 @@ bec_status check_step_error(bec_ctx *ctx)
     int err = 0;
     CKC(step_read_error(ctx->plan, &err, ctx->stream));
     if (err) return fail(ctx, BEC_ERR_CUDA, "fused step: a dependency wait gave up (state of that step is invalid)");
+    if (ctx->pencil_tma && ctx->d_pflags) {
+        CKC(cudaMemcpyAsync(&err, ctx->d_pflags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CKC(cudaStreamSynchronize(ctx->stream));
+        if (err) {
+            CKC(cudaMemsetAsync(ctx->d_pflags, 0, sizeof(int), ctx->stream));   // reported once
+            return fail(ctx, BEC_ERR_CUDA, "TMA pencil pass: a tile load wait gave up (state of that step is invalid)");
+        }
+    }
     return BEC_OK;
 }
 
@@ -1054,6 +1131,8 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
         CKA(dalloc(ctx, &ctx->d_gparams, (size_t)ng));
         CKA(cudaMemcpyAsync(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice, ctx->stream));
         CKA(dalloc(ctx, &ctx->d_step, (size_t)1));
+        CKA(dalloc(ctx, &ctx->d_pflags, (size_t)2));
+        CKA(cudaMemsetAsync(ctx->d_pflags, 0, 2 * sizeof(int), ctx->stream));
         {
             const char *g = std::getenv("BEC_CUDA_GRAPHS");
             ctx->use_graphs = !(g && g[0] == '0');

@@ -196,6 +196,11 @@ void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp,
 // = e^{+i kz_i^2/2 dt frac} for i < nz, then e^{+i (kx^2 + ky^2)/2 dt frac} per pencil (y * nx + x)
 void fp32_kin_tables(float2 *tab, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, float frac,
                      cudaStream_t s);
+// pencil_tma.cu: the non-observing pencil pass as a persistent kernel with TMA tile loads and stores
+// (bit-identical to fp32_pencil_fast); d_err: set to 1 when a wait gave up; d_never: a zero int
+bool fp32_pencil_tma_supported(const ClassGeom &c);
+cudaError_t fp32_pencil_tma(float4 *state, const ClassGeom &c, const float2 *tw_full, float frac, float scale,
+                            const float2 *m, const float2 *kin, int *d_err, const int *d_never, cudaStream_t s);
 int fp32_fast_pencil_tiles(const ClassGeom &c);
 
 // step_kernel.cu: one launch per split step for the classes of the register passes. Items of the work

@@ -108,7 +108,7 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
                 float4 v0[4], o[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const float X = -P.xmax + P.dx * (float)(x + q);
+                    const float X = -P.xmax + P.dx * small_float(x + q);
                     v0[q] = s[c * N + ((x + q) ^ (c & 7))];
                     o[q] = nonlinear_cell(v0[q], 0.5f * (X * X + base), K);
                 }
@@ -182,7 +182,8 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
 #pragma unroll 1
         for (int s = 0; s < 16; s += 2) {
             const int x = kblk(s, h);
-            const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
+            const float xf = small_float(x);
+            const float X0 = -P.xmax + P.dx * xf, X1 = -P.xmax + P.dx * (xf + 1.0f);
             float4 *s0 = tile + tix(r, x), *s1 = tile + tix(r, x + 1);
             const float4 v0 = *s0, v1 = *s1;
             float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
@@ -230,6 +231,86 @@ struct PencilArgs {
     float2 m[4];         // pulse matrix, row-major
 };
 
+// The four-step z transform of a tile of PEN adjacent pencils (nz = 16 G; PEN * G threads), in three
+// stages separated by barriers of the tile's threads. buf holds PEN x NZ float4 (swizzled rows of 16).
+//   inv1:  thread (p, j) = (t % PEN, t / PEN) holds z = j + G m, m < 16: inverse 16-point DFT over
+//          m -> k1, twiddle W^{-j k1}, to buf
+//   mid:   thread (q, p2) = (t % G, t / G) gathers k1 = q + G r (r < 16 / G) for all j: inverse G-point
+//          DFT over j -> k2 (k = k1 + 16 k2), kinetic phase (and pulse), forward G-point DFT, twiddle;
+//          mid_store writes it back after the caller's barrier
+//   fwd3:  thread (p, j) gathers its k1 < 16 and finishes with the forward 16-point DFT over k1 -> m
+template <int NZ, int PEN>
+struct ZTile {
+    static constexpr int R = 16, G = NZ / 16;
+    static_assert(NZ % 16 == 0 && G <= 16, "nz = 16 G with G <= 16");
+
+    __device__ static __forceinline__ int bix(int p, int jj, int k1) { return (p * G + jj) * R + (k1 ^ (p & 7)); }
+
+    __device__ static __forceinline__ void inv1(float4 (&x)[R], float4 *buf, const float2 *tw, int p, int j)
+    {
+        dft<R, true>(x);                                            // over m -> k1 (inverse)
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            const float2 w = tw[j * k1];
+            x[k1] = fftreg::cmulw(x[k1], make_float2(w.x, -w.y));   // W^{-j k1}
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) buf[bix(p, j, k1)] = x[k1];
+    }
+
+    // pxy: the pencil's (kx, ky) factor times the scale; kzp: the kz factors
+    __device__ static __forceinline__ void mid(float4 (&y)[R], const float4 *buf, const float2 *tw, const float2 *kzp,
+                                               float2 pxy, const PencilArgs &pa, int q, int p2)
+    {
+#pragma unroll
+        for (int r = 0; r < R / G; ++r)
+#pragma unroll
+            for (int jj = 0; jj < G; ++jj) y[r * G + jj] = buf[bix(p2, jj, q + G * r)];
+#pragma unroll
+        for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);   // over j -> k2: k = k1 + 16 k2
+
+        // the two unit-modulus factors are applied to the data one after the other: their product, the same
+        // every step for a mode, would round the same way every step and drift the norm of the most
+        // populated modes coherently
+#pragma unroll
+        for (int r = 0; r < R / G; ++r)
+#pragma unroll
+            for (int k2 = 0; k2 < G; ++k2) {
+                const int k = q + G * r + R * k2;
+                float4 v = fftreg::cmulw(fftreg::cmulw(y[r * G + k2], pxy), kzp[k]);
+                if (pa.has_m) {
+                    const float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
+                    const float2 an = cadd(cmul(pa.m[0], a), cmul(pa.m[1], b));
+                    const float2 bn = cadd(cmul(pa.m[2], a), cmul(pa.m[3], b));
+                    v = make_float4(an.x, an.y, bn.x, bn.y);
+                }
+                y[r * G + k2] = v;
+            }
+
+#pragma unroll
+        for (int r = 0; r < R / G; ++r) dft<G, false>(y + r * G); // over k2 -> j (forward)
+#pragma unroll
+        for (int r = 0; r < R / G; ++r)
+#pragma unroll
+            for (int jj = 1; jj < G; ++jj) y[r * G + jj] = fftreg::cmulw(y[r * G + jj], tw[(q + G * r) * jj]);
+    }
+
+    __device__ static __forceinline__ void mid_store(const float4 (&y)[R], float4 *buf, int q, int p2)
+    {
+#pragma unroll
+        for (int r = 0; r < R / G; ++r)
+#pragma unroll
+            for (int jj = 0; jj < G; ++jj) buf[bix(p2, jj, q + G * r)] = y[r * G + jj];
+    }
+
+    __device__ static __forceinline__ void fwd3(float4 (&x)[R], const float4 *buf, int p, int j)
+    {
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[bix(p, j, k1)];
+        dft<R, false>(x);
+    }
+};
+
 // shared memory of one pencil body: 16 pencils x NZ float4, then W_NZ^e, the kz phase and the
 // per-pencil (kx, ky) phase (float2 each)
 template <int NZ>
@@ -246,6 +327,7 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
                                             const PencilArgs &pa, double *__restrict__ obs, float inv_out_scale,
                                             const float2 *__restrict__ kin, float4 *dyn)
 {
+    using Z = ZTile<NZ, 16>;
     constexpr int R = 16, G = NZ / 16;
     (void)gp; (void)tgroup; (void)lx;
     float4 *buf = dyn;                                          // 16 pencils x NZ
@@ -273,7 +355,6 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
         if (t < 16) kxyp[t] = make_float2(1.f, 0.f);
     }
 
-    // stage 1: thread (p, j) holds z = j + G m, m < 16
     const int p = t & 15, j = t >> 4;
     float4 *__restrict__ g = state + (size_t)traj * cells + pen0 + p;
     float4 x[R];
@@ -282,62 +363,17 @@ __device__ __forceinline__ void pencil_body(const VBlock &vb, float4 *__restrict
     copy_async_wait();
     if (t < 16) kxyp[t] = make_float2(pa.scale * kxyp[t].x, pa.scale * kxyp[t].y);
     vb.sync();                                                  // tables ready
-    dft<R, true>(x);                                            // over m -> k1 (inverse)
-#pragma unroll
-    for (int k1 = 1; k1 < R; ++k1) {
-        const float2 w = tw[j * k1];
-        x[k1] = fftreg::cmulw(x[k1], make_float2(w.x, -w.y));   // W^{-j k1}
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) buf[(p * G + j) * R + (k1 ^ (p & 7))] = x[k1];
+    Z::inv1(x, buf, tw, p, j);
     vb.sync();
 
-    // stage 2: thread (q, p2) holds k1 = q + G r (r < 16/G) for all j, then all k2
     const int q = t % G, p2 = t / G;
     float4 y[R];
-#pragma unroll
-    for (int r = 0; r < R / G; ++r)
-#pragma unroll
-        for (int jj = 0; jj < G; ++jj) y[r * G + jj] = buf[(p2 * G + jj) * R + ((q + G * r) ^ (p2 & 7))];
-#pragma unroll
-    for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);   // over j -> k2: k = k1 + 16 k2
-
-    // the two unit-modulus factors are applied to the data one after the other: their product, the same
-    // every step for a mode, would round the same way every step and drift the norm of the most
-    // populated modes coherently
-    const float2 pxy = kxyp[p2];
-#pragma unroll
-    for (int r = 0; r < R / G; ++r)
-#pragma unroll
-        for (int k2 = 0; k2 < G; ++k2) {
-            const int k = q + G * r + R * k2;
-            float4 v = fftreg::cmulw(fftreg::cmulw(y[r * G + k2], pxy), kzp[k]);
-            if (pa.has_m) {
-                const float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
-                const float2 an = cadd(cmul(pa.m[0], a), cmul(pa.m[1], b));
-                const float2 bn = cadd(cmul(pa.m[2], a), cmul(pa.m[3], b));
-                v = make_float4(an.x, an.y, bn.x, bn.y);
-            }
-            y[r * G + k2] = v;
-        }
-
-#pragma unroll
-    for (int r = 0; r < R / G; ++r) dft<G, false>(y + r * G); // over k2 -> j (forward)
-#pragma unroll
-    for (int r = 0; r < R / G; ++r)
-#pragma unroll
-        for (int jj = 1; jj < G; ++jj) y[r * G + jj] = fftreg::cmulw(y[r * G + jj], tw[(q + G * r) * jj]);
+    Z::mid(y, buf, tw, kzp, kxyp[p2], pa, q, p2);
     vb.sync();                                                  // stage-2 reads done
-#pragma unroll
-    for (int r = 0; r < R / G; ++r)
-#pragma unroll
-        for (int jj = 0; jj < G; ++jj) buf[(p2 * G + jj) * R + ((q + G * r) ^ (p2 & 7))] = y[r * G + jj];
+    Z::mid_store(y, buf, q, p2);
     vb.sync();
 
-    // stage 3: thread (p, j) gathers k1 < 16 and finishes over k1 -> m
-#pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[(p * G + j) * R + (k1 ^ (p & 7))];
-    dft<R, false>(x);
+    Z::fwd3(x, buf, p, j);
     if constexpr (OBS) {
         // the output is out_scale * FFT_z(boundary state); undo the scale for the moments
         vb.sync();                                              // stage-3 reads of buf done

@@ -1,11 +1,14 @@
-"""The fused step kernel (one persistent launch per split step) and its autotuned work list.
+"""The split-step schedules: per-pass launches (plane passes at 16 or 20 warps per SM, pencil passes on
+the register kernel or the persistent TMA kernel) and the fused step kernel (one persistent launch per
+split step) on its autotuned work list.
 
-Every schedule computes the same bits: launches per pass and grid class, the two-phase work list, and
-the interleaved work lists at every distance, with samples, a pi pulse, captured step graphs and a
-grid class that the fused kernel does not take (a 2D slice). The autotuner picks one of the
-candidates and reports its timings; a steady step of the fused classes is one launch. A dependency wait
-that runs out (a plane item told to wait for one pencil item more than exists) ends with BEC_ERR_CUDA
-and leaves the device usable.
+Every schedule computes the same bits: launches per pass and grid class, with either pencil kernel, the
+two-phase work list, and the interleaved work lists at every distance, with samples, a pi pulse, captured
+step graphs and a grid class that the fused kernel does not take (a 2D slice). The autotuner picks one of
+the candidates and reports its timings; a steady step of the fused classes is one launch. A dependency
+wait that runs out (a plane item told to wait for one pencil item more than exists), and a TMA tile wait
+that runs out (the first tile of every CTA also waiting for a flag that nothing sets), end with
+BEC_ERR_CUDA and leave the device usable.
 """
 import numpy as np
 import pytest
@@ -24,6 +27,10 @@ GROUPS = [
     rb87_params(N=25000, grid=(32, 1, 128), ne=2, noise=True, seed=54),
     rb87_params(N=20000, grid=(16, 16, 64), ne=1, noise=True, seed=55),
 ]
+
+
+PER_PASS = ["unfused", "unfused-20", "unfused-tma", "unfused-20-tma"]
+N_CANDIDATES = len(PER_PASS) + 5
 
 
 @pytest.fixture(scope="module")
@@ -51,16 +58,17 @@ def _run(monkeypatch, plan, gss, groups=GROUPS):
 def test_every_schedule_gives_the_same_bits(monkeypatch, ground_states):
     ref = _run(monkeypatch, "unfused", ground_states)
     assert ref["plan"]["candidate"] == 0 and ref["plan"]["fused_classes"] == 0
-    for plan in ["unfused-20", "0", "1", "2", "3", "4", None]:
+    for plan in PER_PASS[1:] + ["0", "1", "2", "3", "4", None]:
         got = _run(monkeypatch, plan, ground_states)
         p = got["plan"]
         if plan is None:
-            assert p["chosen"] in ("autotuned", "cached") and 0 <= p["candidate"] < 7
-        elif plan == "unfused-20":
-            assert p["chosen"] == "forced" and p["candidate"] == 1
+            assert p["chosen"] in ("autotuned", "cached") and 0 <= p["candidate"] < N_CANDIDATES
+        elif plan in PER_PASS:
+            assert p["chosen"] == "forced" and p["candidate"] == PER_PASS.index(plan)
         else:
-            assert p["chosen"] == "forced" and p["candidate"] == int(plan) + 2
-        assert p["fused_classes"] == (4 if p["candidate"] >= 2 else 0)    # every class but the 2D slice
+            assert p["chosen"] == "forced" and p["candidate"] == int(plan) + len(PER_PASS)
+        # the fused kernel takes every class but the 2D slice
+        assert p["fused_classes"] == (4 if p["candidate"] >= len(PER_PASS) else 0)
         np.testing.assert_array_equal(got["mom"], ref["mom"])
         np.testing.assert_array_equal(got["now"], ref["now"])
         for a, b in zip(got["states"], ref["states"]):
@@ -82,11 +90,16 @@ def test_autotuner_reports_timings(monkeypatch, ground_states):
     eng, _ = _three_classes(ground_states)
     p = eng.step_plan
     assert p["chosen"] in ("autotuned", "cached")
-    assert len(p["candidates"]) == 7
+    assert len(p["candidates"]) == N_CANDIDATES
     if p["chosen"] == "autotuned":
-        ms = p["candidate_ms_per_step"]           # per-pass launches at 16 and 20 warps per SM, the work lists 0..4
-        assert len(ms) == 7 and all(v > 0 for v in ms)
+        ms = p["candidate_ms_per_step"]           # the four per-pass schedules, the work lists 0..4
+        assert len(ms) == N_CANDIDATES and all(v > 0 for v in ms)
         assert ms[p["candidate"]] == min(ms)
+        # per grid class, the faster pencil kernel (register or TMA) was timed and is the one the TMA
+        # schedules use
+        for k in p["pencil_kernels"]:
+            assert k["register_ms"] > 0 and k["tma_ms"] > 0
+            assert k["tma"] == (p["candidate"] in (2, 3) and k["tma_ms"] < k["register_ms"])
 
 
 def test_fused_plan_is_one_launch_per_step(monkeypatch, ground_states):
@@ -117,3 +130,22 @@ def test_dependency_wait_that_runs_out_is_reported(monkeypatch, ground_states):
     got = _run(monkeypatch, "2", ground_states[:1], groups=[GROUPS[0]])
     ref = _run(monkeypatch, "unfused", ground_states[:1], groups=[GROUPS[0]])
     np.testing.assert_array_equal(got["mom"], ref["mom"])
+
+
+def test_tma_tile_wait_that_runs_out_is_reported(monkeypatch, ground_states):
+    monkeypatch.setenv("BEC_STEP_PLAN", "unfused-tma")
+    monkeypatch.setenv("BEC_STEP_WAIT_LIMIT_MS", "20")
+    monkeypatch.setenv("BEC_PENCIL_INJECT_STALL", "1")
+    eng = Engine([GROUPS[2]], path=BEC_PATH_FP32_BATCHED)
+    eng.init_group(0, ground_states[2])
+    with pytest.raises(BecError) as ei:
+        eng.start_evolution()
+    assert ei.value.status == BEC_ERR_CUDA and "wait" in str(ei.value)
+    eng.close()
+    monkeypatch.delenv("BEC_PENCIL_INJECT_STALL")
+    monkeypatch.delenv("BEC_STEP_WAIT_LIMIT_MS")
+    got = _run(monkeypatch, "unfused-tma", ground_states[2:3], groups=[GROUPS[2]])
+    ref = _run(monkeypatch, "unfused", ground_states[2:3], groups=[GROUPS[2]])
+    np.testing.assert_array_equal(got["mom"], ref["mom"])
+    for a, b in zip(got["states"], ref["states"]):
+        np.testing.assert_array_equal(a, b)
