@@ -50,6 +50,11 @@ struct GroupRec {
     bool initialised = false;
 };
 
+// the pencil kernels of the per-pass schedule: register (fused_passes.cu k_pencil), persistent TMA
+// (pencil_tma.cu)
+constexpr int kPencilRegister = 0, kPencilTma = 1, kPencilKinds = 2;
+const char *const kPencilNames[kPencilKinds] = {"register", "tma"};
+
 struct ClassRec {
     ClassGeom geom{};
     float4 *state = nullptr;
@@ -62,8 +67,8 @@ struct ClassRec {
     int traj_offset = 0;      // global index of the class's first trajectory
     std::vector<int> groups;  // group indices in this class
     float2 *kin_tab[2] = {nullptr, nullptr};   // kinetic phase tables for kick fractions 0.5 and 1 (register pencils)
-    bool tma_pick = true;     // the TMA pencil schedules use the TMA kernel for this class (autotuned per class)
-    double pencil_ms[2] = {-1.0, -1.0};        // autotuner: register / TMA pencil pass, ms per launch
+    int pencil_kind = 0;      // the tuned per-pass schedules' pencil kernel for this class (kPencilRegister ...)
+    double pencil_ms[2] = {-1.0, -1.0};        // autotuner: ms per launch of each pencil kernel
 };
 
 } // namespace
@@ -85,7 +90,7 @@ struct bec_ctx {
     std::vector<char> fused;             // per class: 1 when its passes run in the fused step
     int plan_mode = -2;                  // -2: not chosen yet, else the schedule candidate (ensure_plan)
     int plane_occupancy = 0;             // per-pass plane launches: 0 = 16 warps per SM, 1 = 20
-    bool pencil_tma = false;             // per-pass pencil launches: the persistent TMA kernel (pencil_tma.cu)
+    bool pencil_tuned = false;           // per-pass pencil launches: each class's own pencil kernel (pencil_kind)
     int *d_pflags = nullptr;             // batched: [0] error flag of the TMA pencil pass, [1] a flag nothing sets
     std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
@@ -399,7 +404,8 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
             if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
             const float frac = kf;
             const float2 *kin = frac == 1.0f ? c.kin_tab[1] : frac == 0.5f ? c.kin_tab[0] : nullptr;
-            if (!observe && ctx->pencil_tma && c.tma_pick && fp32_pencil_tma_supported(c.geom))
+            const int kind = !observe && ctx->pencil_tuned ? c.pencil_kind : kPencilRegister;
+            if (kind == kPencilTma && fp32_pencil_tma_supported(c.geom))
                 CKC(fp32_pencil_tma(c.state, c.geom, twf, frac, z.scale * z.out_scale, mf, kin, ctx->d_pflags,
                                     ctx->d_pflags + 1, ctx->stream));
             else
@@ -477,46 +483,46 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
 // The split-step schedule of a batched context, chosen once before its first step. Candidates:
 //   0  per-pass launches, plane passes at 16 warps per SM (no register spill)
 //   1  per-pass launches, plane passes at 20 warps per SM (96 registers, a small spill)
-//   2, 3  as 0, 1 with the non-observing pencil passes on the persistent TMA kernel
+//   2, 3  as 0, 1 with each class's non-observing pencil pass on the faster pencil kernel (pick_pencil_kernels)
 //   4 + k  the fused step kernel on work list k (two-phase, interleaved at 0.5, 1, 2, 4 waves)
-// BEC_STEP_PLAN in the environment forces one ("unfused" = 0, "unfused-20" = 1, "unfused-tma" = 2,
-// "unfused-20-tma" = 3, "0".."4" = fused k); otherwise a choice cached for the same class mix on this
-// device is reused, or every candidate is timed on a copy of the state (BEC_AUTOTUNE=0 skips the timing
-// and takes candidate 0).
+// BEC_STEP_PLAN in the environment forces one ("unfused" = 0, "unfused-20" = 1, "unfused-tma" = 2 and
+// "unfused-20-tma" = 3 with every class on the TMA pencil kernel, "0".."4" = fused k); otherwise a choice
+// cached for the same class mix on this device is reused, or every candidate is timed on a copy of the state
+// (BEC_AUTOTUNE=0 skips the timing and takes candidate 0).
 constexpr int kPerPassCandidates = 4;
 constexpr int kAllCandidates = kPerPassCandidates + kStepCandidates;
 const char *const kPerPassNames[kPerPassCandidates] = {"unfused", "unfused-20", "unfused-tma", "unfused-20-tma"};
+constexpr size_t kPickClasses = 12;   // classes whose pencil picks the plan cache keeps
 
 std::string candidate_name(int c)
 {
     if (c < kPerPassCandidates)
         return std::string("per-pass launches, ") + (c & 1 ? "20" : "16") + " warps per SM" +
-               (c >= 2 ? ", TMA pencil pass" : "");
+               (c >= 2 ? ", pencil kernel tuned per class" : "");
     return std::string("fused ") + step_plan_name(c - kPerPassCandidates);
 }
 
 bec_status check_step_error(bec_ctx *ctx);
 
 // Per grid class, the faster of the two pencil kernels for the full-kick pass of a steady step: the register
-// kernel (16 pencils per CTA, two CTAs per SM) or the persistent TMA kernel (three CTAs per SM, the next
-// tile's load in flight). Both compute the same bits; each is timed over three launches after one warm-up on
-// the current state (the caller restores it).
+// kernel (16 pencils per CTA of nz threads, 16 warps per SM) or the persistent TMA kernel (three CTAs per SM,
+// the next tile's load in flight). Both compute the same bits; each is timed over three launches after one
+// warm-up on the current state (the caller restores it).
 bec_status pick_pencil_kernels(bec_ctx *ctx)
 {
     for (auto &c : ctx->classes) {
-        c.tma_pick = true;
+        c.pencil_kind = kPencilRegister;
         c.pencil_ms[0] = c.pencil_ms[1] = -1.0;
-        if (c.geom.n_traj == 0 || !ctx->use_fast || !fp32_fast_pencil_supported(c.geom) ||
-            !fp32_pencil_tma_supported(c.geom) || !c.kin_tab[1])
-            continue;
+        if (c.geom.n_traj == 0 || !ctx->use_fast || !fp32_fast_pencil_supported(c.geom) || !c.kin_tab[1]) continue;
         float2 *twf;
         bec_status st;
         if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
         const float scale = (float)(1.0 / (double)c.geom.cells);
-        for (int kind = 0; kind < 2; ++kind) {
+        for (int kind = 0; kind < kPencilKinds; ++kind) {
+            if (kind == kPencilTma && !fp32_pencil_tma_supported(c.geom)) continue;
             for (int r = 0; r < 4; ++r) {
                 if (r == 1) CKC(cudaEventRecord(ctx->ev0, ctx->stream));
-                if (kind == 0)
+                if (kind == kPencilRegister)
                     fp32_pencil_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, twf, 1.0f, scale, nullptr, nullptr,
                                      1.0f, c.kin_tab[1], ctx->stream);
                 else
@@ -528,8 +534,8 @@ bec_status pick_pencil_kernels(bec_ctx *ctx)
             float ms = 0.f;
             CKC(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
             c.pencil_ms[kind] = ms / 3.0;
+            if (c.pencil_ms[kind] < c.pencil_ms[c.pencil_kind]) c.pencil_kind = kind;
         }
-        c.tma_pick = c.pencil_ms[1] < c.pencil_ms[0];
     }
     return BEC_OK;
 }
@@ -570,14 +576,14 @@ bec_status ensure_plan(bec_ctx *ctx)
         if (c < kPerPassCandidates) {
             ctx->plan.ready = false;
             ctx->plane_occupancy = c & 1;
-            ctx->pencil_tma = c >= 2;
+            ctx->pencil_tuned = c >= 2;
             for (int ci : idx) ctx->fused[ci] = 0;
             return BEC_OK;
         }
         if (step_plan_build(ctx->plan, geoms, devs, offs, c - kPerPassCandidates, ctx->stream) != cudaSuccess)
             return fail(ctx, BEC_ERR_CUDA, "fused step plan");
         ctx->plane_occupancy = 0;
-        ctx->pencil_tma = false;
+        ctx->pencil_tuned = false;
         for (int ci : idx) ctx->fused[ci] = 1;
         return BEC_OK;
     };
@@ -587,7 +593,8 @@ bec_status ensure_plan(bec_ctx *ctx)
     bec_status st;
     const int named = (int)(std::find(kPerPassNames, kPerPassNames + kPerPassCandidates, fs) - kPerPassNames);
     if (named < kPerPassCandidates) {
-        cand = named;
+        cand = named;                                  // "-tma": every class on the TMA pencil kernel
+        for (auto &c : ctx->classes) c.pencil_kind = named < 2 ? kPencilRegister : kPencilTma;
         how = "forced";
     } else if (!fs.empty()) {
         const int k = std::atoi(fs.c_str());
@@ -596,8 +603,9 @@ bec_status ensure_plan(bec_ctx *ctx)
         cand = kPerPassCandidates + k;
         how = "forced";
     } else if (step_plan_cached(geoms, &cand)) {
-        // the candidate, and above bit 8 the per-class pencil kernel picks
-        for (size_t ci = 0; ci < ctx->classes.size() && ci < 23; ++ci) ctx->classes[ci].tma_pick = (cand >> (8 + ci)) & 1;
+        // the candidate, and above bit 8 two bits per class: its pencil kernel
+        for (size_t ci = 0; ci < ctx->classes.size() && ci < kPickClasses; ++ci)
+            ctx->classes[ci].pencil_kind = (cand >> (8 + 2 * ci)) & 3;
         cand &= 0xFF;
         how = "cached";
     } else {
@@ -650,8 +658,8 @@ bec_status ensure_plan(bec_ctx *ctx)
                 if ((st = check_step_error(ctx))) return st;
                 how = "autotuned";
                 int picks = 0;
-                for (size_t ci = 0; ci < ctx->classes.size() && ci < 23; ++ci)
-                    picks |= (ctx->classes[ci].tma_pick ? 1 : 0) << (8 + ci);
+                for (size_t ci = 0; ci < ctx->classes.size() && ci < kPickClasses; ++ci)
+                    picks |= ctx->classes[ci].pencil_kind << (8 + 2 * ci);
                 step_plan_remember(geoms, cand | picks);
             } else {
                 cudaGetLastError();
@@ -675,10 +683,11 @@ bec_status ensure_plan(bec_ctx *ctx)
     bool firstc = true;
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
-        std::snprintf(buf, sizeof buf, "%s{\"grid\": [%d, %d, %d], \"tma\": %s, \"register_ms\": %.4f, \"tma_ms\": %.4f}",
-                      firstc ? "" : ", ", c.geom.nx, c.geom.ny, c.geom.nz,
-                      ctx->pencil_tma && c.tma_pick && fp32_pencil_tma_supported(c.geom) ? "true" : "false",
-                      c.pencil_ms[0], c.pencil_ms[1]);
+        const int kind = ctx->pencil_tuned ? c.pencil_kind : kPencilRegister;
+        std::snprintf(buf, sizeof buf,
+                      "%s{\"grid\": [%d, %d, %d], \"kernel\": \"%s\", \"register_ms\": %.4f, \"tma_ms\": %.4f}",
+                      firstc ? "" : ", ", c.geom.nx, c.geom.ny, c.geom.nz, kPencilNames[kind], c.pencil_ms[0],
+                      c.pencil_ms[1]);
         j += buf;
         firstc = false;
     }
@@ -747,7 +756,7 @@ bec_status check_step_error(bec_ctx *ctx)
     int err = 0;
     CKC(step_read_error(ctx->plan, &err, ctx->stream));
     if (err) return fail(ctx, BEC_ERR_CUDA, "fused step: a dependency wait gave up (state of that step is invalid)");
-    if (ctx->pencil_tma && ctx->d_pflags) {
+    if (ctx->pencil_tuned && ctx->d_pflags) {
         CKC(cudaMemcpyAsync(&err, ctx->d_pflags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CKC(cudaStreamSynchronize(ctx->stream));
         if (err) {

@@ -68,13 +68,16 @@ __device__ __forceinline__ float4 add(float4 a, float4 b) { return make_float4(a
 __device__ __forceinline__ float4 sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
 
 // v * (c + i s)
+// Complex products with the fused multiply-adds written out, so that a float2 and a float4 caller round
+// every component the same way (left to the compiler, the contraction of a*b - c*d can differ between them).
 __device__ __forceinline__ float2 cmulc(float2 v, float c, float s)
 {
-    return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+    return make_float2(fmaf(v.x, c, -(v.y * s)), fmaf(v.x, s, v.y * c));
 }
 __device__ __forceinline__ float4 cmulc(float4 v, float c, float s)
 {
-    return make_float4(v.x * c - v.y * s, v.x * s + v.y * c, v.z * c - v.w * s, v.z * s + v.w * c);
+    const float2 a = cmulc(make_float2(v.x, v.y), c, s), b = cmulc(make_float2(v.z, v.w), c, s);
+    return make_float4(a.x, a.y, b.x, b.y);
 }
 // v * (-i)
 __device__ __forceinline__ float2 mul_negi(float2 v) { return make_float2(v.y, -v.x); }
@@ -84,10 +87,13 @@ __device__ __forceinline__ float2 mul_posi(float2 v) { return make_float2(-v.y, 
 __device__ __forceinline__ float4 mul_posi(float4 v) { return make_float4(-v.y, v.x, -v.w, v.z); }
 
 // v * w with w a runtime complex (float2)
-__device__ __forceinline__ float2 cmulw(float2 v, float2 w) { return make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x); }
-__device__ __forceinline__ float4 cmulw(float4 v, float2 w)
+__device__ __forceinline__ float2 cmulw(float2 v, float2 w) { return cmulc(v, w.x, w.y); }
+__device__ __forceinline__ float4 cmulw(float4 v, float2 w) { return cmulc(v, w.x, w.y); }
+// m0 a + m1 b, every rounding fixed
+__device__ __forceinline__ float2 cmix(float2 m0, float2 a, float2 m1, float2 b)
 {
-    return make_float4(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x, v.z * w.x - v.w * w.y, v.z * w.y + v.w * w.x);
+    return make_float2(fmaf(m0.x, a.x, fmaf(-m0.y, a.y, fmaf(m1.x, b.x, -(m1.y * b.y)))),
+                       fmaf(m0.x, a.y, fmaf(m0.y, a.x, fmaf(m1.x, b.y, m1.y * b.x))));
 }
 
 // ---- butterfly with a constant twiddle -------------------------------------------

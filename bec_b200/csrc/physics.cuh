@@ -47,27 +47,17 @@ __device__ __forceinline__ CellConsts cell_consts(const GroupParamsF &P)
     return K;
 }
 
-// (f + 1/2) / 2^21 and f / 2^21 of a 21-bit field f, exact: f becomes mantissa bits 2..22 of a float in
-// [1, 2) (bit 1 set for the half) and the 1 is subtracted -- an ALU op and an add instead of an
-// integer-to-float conversion, which shares the SFU's quarter-rate pipe with the log2/sqrt/sin/cos below.
-__device__ __forceinline__ float open21(uint32_t f) { return __uint_as_float(0x3F800002u | (f << 2)) - 1.0f; }
-__device__ __forceinline__ float frac21(uint32_t f) { return __uint_as_float(0x3F800000u | (f << 2)) - 1.0f; }
-
-// A small non-negative integer (< 2^23) as a float, exact, by the same construction.
-__device__ __forceinline__ float small_float(int i) { return __uint_as_float(0x4B000000u | (uint32_t)i) - 8388608.0f; }
-
 // One Box-Muller pair of loss_normals6 scaled by an amplitude amp, with the SFU log2/sqrt/sin/cos:
 // r = amp sqrt(-2 ln u1) = sqrt(n log2 u1) for n = -2 ln 2 amp^2, u1 = (f1 + 1/2) / 2^21 in (0, 1);
-// (n1, n2) = r (cos, sin)(2 pi f2 / 2^21), the angle rounded once from the exact f2 / 2^21 times
-// fl(2 pi). log2 u1 < 0 for every u1 here: its largest value, log2(1 - 2^-22) = -3.4e-7, is twice the
-// SFU log2's absolute error bound on [0.5, 2].
+// (n1, n2) = r (cos, sin)(2 pi f2 / 2^21). log2 u1 < 0 for every u1 here: its largest value,
+// log2(1 - 2^-22) = -3.4e-7, is twice the SFU log2's absolute error bound on [0.5, 2].
 __device__ __forceinline__ float2 box_muller21_scaled(uint32_t f1, uint32_t f2, float n)
 {
-    const float y = n * __log2f(open21(f1));
+    const float y = n * __log2f(fmaf((float)f1, 0x1p-21f, 0x1p-22f));
     float r;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
     float s, c;
-    __sincosf(frac21(f2) * 6.28318530717958648f, &s, &c);
+    __sincosf((float)f2 * (6.28318530717958648f * 0x1p-21f), &s, &c);
     return make_float2(r * c, r * s);
 }
 

@@ -108,7 +108,7 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
                 float4 v0[4], o[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const float X = -P.xmax + P.dx * small_float(x + q);
+                    const float X = -P.xmax + P.dx * (float)(x + q);
                     v0[q] = s[c * N + ((x + q) ^ (c & 7))];
                     o[q] = nonlinear_cell(v0[q], 0.5f * (X * X + base), K);
                 }
@@ -182,8 +182,7 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
 #pragma unroll 1
         for (int s = 0; s < 16; s += 2) {
             const int x = kblk(s, h);
-            const float xf = small_float(x);
-            const float X0 = -P.xmax + P.dx * xf, X1 = -P.xmax + P.dx * (xf + 1.0f);
+            const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
             float4 *s0 = tile + tix(r, x), *s1 = tile + tix(r, x + 1);
             const float4 v0 = *s0, v1 = *s1;
             float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
@@ -280,8 +279,8 @@ struct ZTile {
                 float4 v = fftreg::cmulw(fftreg::cmulw(y[r * G + k2], pxy), kzp[k]);
                 if (pa.has_m) {
                     const float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
-                    const float2 an = cadd(cmul(pa.m[0], a), cmul(pa.m[1], b));
-                    const float2 bn = cadd(cmul(pa.m[2], a), cmul(pa.m[3], b));
+                    const float2 an = fftreg::cmix(pa.m[0], a, pa.m[1], b);
+                    const float2 bn = fftreg::cmix(pa.m[2], a, pa.m[3], b);
                     v = make_float4(an.x, an.y, bn.x, bn.y);
                 }
                 y[r * G + k2] = v;

@@ -1,8 +1,8 @@
-"""The split-step schedules: per-pass launches (plane passes at 16 or 20 warps per SM, pencil passes on
-the register kernel or the persistent TMA kernel) and the fused step kernel (one persistent launch per
-split step) on its autotuned work list.
+"""The split-step schedules: per-pass launches (plane passes at 16 or 20 warps per SM; pencil passes on the
+register kernel or the persistent TMA kernel, chosen per grid class) and the
+fused step kernel (one persistent launch per split step) on its autotuned work list.
 
-Every schedule computes the same bits: launches per pass and grid class, with either pencil kernel, the
+Every schedule computes the same bits: launches per pass and grid class, with any pencil kernel, the
 two-phase work list, and the interleaved work lists at every distance, with samples, a pi pulse, captured
 step graphs and a grid class that the fused kernel does not take (a 2D slice). The autotuner picks one of
 the candidates and reports its timings; a steady step of the fused classes is one launch. A dependency
@@ -29,8 +29,11 @@ GROUPS = [
 ]
 
 
-PER_PASS = ["unfused", "unfused-20", "unfused-tma", "unfused-20-tma"]
-N_CANDIDATES = len(PER_PASS) + 5
+# forced per-pass schedules and their candidate numbers: register pencils at 16 / 20 warps per SM, then every class
+# on the TMA pencil kernel
+PER_PASS = {"unfused": 0, "unfused-20": 1, "unfused-tma": 2, "unfused-20-tma": 3}
+N_PER_PASS = 4
+N_CANDIDATES = N_PER_PASS + 5
 
 
 @pytest.fixture(scope="module")
@@ -58,17 +61,19 @@ def _run(monkeypatch, plan, gss, groups=GROUPS):
 def test_every_schedule_gives_the_same_bits(monkeypatch, ground_states):
     ref = _run(monkeypatch, "unfused", ground_states)
     assert ref["plan"]["candidate"] == 0 and ref["plan"]["fused_classes"] == 0
-    for plan in PER_PASS[1:] + ["0", "1", "2", "3", "4", None]:
+    for plan in list(PER_PASS)[1:] + ["0", "1", "2", "3", "4", None]:
         got = _run(monkeypatch, plan, ground_states)
         p = got["plan"]
         if plan is None:
             assert p["chosen"] in ("autotuned", "cached") and 0 <= p["candidate"] < N_CANDIDATES
         elif plan in PER_PASS:
-            assert p["chosen"] == "forced" and p["candidate"] == PER_PASS.index(plan)
+            assert p["chosen"] == "forced" and p["candidate"] == PER_PASS[plan]
+            want = "tma" if plan.endswith("tma") else "register"
+            assert all(k["kernel"] == want for k in p["pencil_kernels"])
         else:
-            assert p["chosen"] == "forced" and p["candidate"] == int(plan) + len(PER_PASS)
+            assert p["chosen"] == "forced" and p["candidate"] == int(plan) + N_PER_PASS
         # the fused kernel takes every class but the 2D slice
-        assert p["fused_classes"] == (4 if p["candidate"] >= len(PER_PASS) else 0)
+        assert p["fused_classes"] == (4 if p["candidate"] >= N_PER_PASS else 0)
         np.testing.assert_array_equal(got["mom"], ref["mom"])
         np.testing.assert_array_equal(got["now"], ref["now"])
         for a, b in zip(got["states"], ref["states"]):
@@ -95,11 +100,11 @@ def test_autotuner_reports_timings(monkeypatch, ground_states):
         ms = p["candidate_ms_per_step"]           # the four per-pass schedules, the work lists 0..4
         assert len(ms) == N_CANDIDATES and all(v > 0 for v in ms)
         assert ms[p["candidate"]] == min(ms)
-        # per grid class, the faster pencil kernel (register or TMA) was timed and is the one the TMA
-        # schedules use
+        # per grid class, both pencil kernels were timed, and the tuned schedules use the faster
         for k in p["pencil_kernels"]:
-            assert k["register_ms"] > 0 and k["tma_ms"] > 0
-            assert k["tma"] == (p["candidate"] in (2, 3) and k["tma_ms"] < k["register_ms"])
+            ms = {name: k[name + "_ms"] for name in ("register", "tma")}
+            assert all(v > 0 for v in ms.values())
+            assert k["kernel"] == (min(ms, key=ms.get) if p["candidate"] in (2, 3) else "register")
 
 
 def test_fused_plan_is_one_launch_per_step(monkeypatch, ground_states):
