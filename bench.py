@@ -143,15 +143,40 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def mix_sample(groups, n):
+    """n trajectories of groups (one trajectory per group) with the batch's share of every grid class, so that a
+    sample's traj-steps/s compare with the whole batch's (the first ones of each class, in batch order)."""
+    by = {}
+    for p in groups:
+        by.setdefault((p.nvx, p.nvy, p.nvz), []).append(p)
+    n = min(n, len(groups))
+    share = {k: n * len(v) / len(groups) for k, v in by.items()}
+    take = {k: int(x) for k, x in share.items()}
+    for k in sorted(share, key=lambda q: take[q] - share[q])[:n - sum(take.values())]:
+        take[k] += 1                                   # largest remainders first
+    out, used = [], {k: 0 for k in take}
+    for p in groups:
+        k = (p.nvx, p.nvy, p.nvz)
+        if used[k] < take[k]:
+            out.append(p)
+            used[k] += 1
+    return out
+
+
+def mean_cells(groups):
+    return sum(p.nvx * p.nvy * p.nvz * p.ne for p in groups) / max(1, sum(p.ne for p in groups))
+
+
 class OracleSample:
     """A bounded sample of the workload on the CPU oracle (FP64 restatement of the
-    reference's split step), one trajectory per thread on all host cores."""
+    reference's split step), one trajectory per thread on all host cores; the sample has the
+    workload's grid-class mix."""
 
     def __init__(self, groups):
         from concurrent.futures import ThreadPoolExecutor
         from oracle import oracle as O
         self.cores = os.cpu_count() or 1
-        self.sample = groups[:max(3, min(len(groups), 2 * self.cores))]
+        self.sample = mix_sample(groups, max(3, 2 * self.cores))
         self.ens = []
         for p in self.sample:
             e = O.OracleEnsemble(p)
@@ -423,15 +448,16 @@ def main():
     extras = {}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_extras:
-        # plain per-trajectory FP64 path on a sample with the same grid mix
-        sample = groups[:24]
+        # plain per-trajectory FP64 path on a sample with the batch's grid mix
+        sample = mix_sample(groups, 24)
         plain = Engine(sample, path=BEC_PATH_FP64_PLAIN)
         for g, d in enumerate(plain.derived):
             plain.init_group(g, thomas_fermi(d))
         plain.start_evolution()
-        plain.evolve(1)
         plain.evolve(2)
-        pv = len(sample) * 2 / (plain.last_device_ms * 1e-3)
+        plain_steps = 20
+        plain.evolve(plain_steps)
+        pv = len(sample) * plain_steps / (plain.last_device_ms * 1e-3)
         # the batched path on the same sample, for the like-for-like ratio
         bs = Engine(sample, path=BEC_PATH_FP32_BATCHED)
         for g, d in enumerate(bs.derived):
@@ -440,13 +466,18 @@ def main():
         bs.evolve(3)
         bs.evolve(10)
         bv = len(sample) * 10 / (bs.last_device_ms * 1e-3)
-        extras["plain_fp64"] = {"value": pv, "unit": "traj-steps/s", "sample": f"{len(sample)} trajectories, 2 steps",
+        mix = {}
+        for p in sample:
+            mix[f"{p.nvx}x{p.nvy}x{p.nvz}"] = mix.get(f"{p.nvx}x{p.nvy}x{p.nvz}", 0) + 1
+        extras["plain_fp64"] = {"value": pv, "unit": "traj-steps/s",
+                                "sample": f"{len(sample)} trajectories of the workload mix {mix}, {plain_steps} steps",
                                 "batched_fp32_same_sample": bv, "ratio_same_sample": bv / pv,
                                 "ratio_full_batch": value / pv}
         plain.close()
         bs.close()
         v, cores, s = cpu_baseline(groups, args.cpu_seconds)
-        cpu = {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": s}
+        cpu = {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": s,
+               "cell_steps_per_s": v * mean_cells(mix_sample(groups, max(3, 2 * cores)))}
     if rank == 0 and ws == 1 and not args.no_extras and not args.no_gs:
         extras["gs_warmstart"] = gs_warmstart_leg(args.gs_train, args.gs_eval, GS_TOL, GS_REF_TOL)
 
@@ -467,7 +498,8 @@ def main():
         line = {
             "metric": "wigner_traj_steps_per_s", "value": value, "unit": "traj-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms / args.steps, "cell_steps_per_s": value * mean_cells(all_groups),
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD if not args.grids else f"{args.n_traj}x{args.grids}",
                        "n_traj_per_gpu": args.n_traj,

@@ -364,11 +364,14 @@ int32_t bec_step_graphs(const bec_ctx *ctx);
  * run it together as ONE launch of a persistent kernel walking a work list of pencil-pass and
  * plane-pass items (a trajectory's plane items wait on its pencil items). Before the context's
  * first step an autotuner times the candidates on a copy of the state -- per-pass launches with
- * the plane passes at 16 or at 20 warps per SM, and the work list run in two phases or
- * interleaving each trajectory's plane items 0.5 to 4 waves of the grid after its pencil items --
- * and keeps the fastest for this class mix and device (cached per process). BEC_STEP_PLAN in the
- * environment forces one (unfused, unfused-20, or 0..4 for the work lists), BEC_AUTOTUNE=0 takes
- * the per-pass launches untimed; every schedule computes the same bits. The reference has one fixed
+ * the plane passes at 16 or at 20 warps per SM, each with the register pencil kernel or with every
+ * class's pencil pass on the faster of the register kernel and a persistent TMA kernel (timed per
+ * class: "pencil_kernels" in the JSON), and the work list run in two phases or interleaving each
+ * trajectory's plane items 0.5 to 4 waves of the grid after its pencil items -- and keeps the
+ * fastest for this class mix and device (cached per process). BEC_STEP_PLAN in the environment
+ * forces one (unfused, unfused-20, unfused-tma and unfused-20-tma with every class on the TMA
+ * pencil kernel, or 0..4 for the work lists), BEC_AUTOTUNE=0 takes the per-pass launches untimed;
+ * every schedule computes the same bits. The reference has one fixed
  * schedule of eight launches per ensemble and step (wigner.cu:178-199) with cuFFT plans built by
  * batchfftPlan3d (batchfft.cu:22-100). */
 bec_status bec_step_plan(bec_ctx *ctx, char *out, int32_t len);
