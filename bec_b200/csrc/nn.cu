@@ -6,9 +6,10 @@
 // which alone decides convergence.
 //
 // Layers are Y = act(X W^T + b) (W is [out x in], row-major, as a linear layer),
-// tanh on hidden layers, identity on the last. GEMMs run on the tensor cores with
-// BF16 operands and FP32 accumulation (mma.sync m16n8k16); master weights, Adam
-// moments, activations' pre-images and gradients are FP32.
+// tanh on hidden layers, identity on the last. GEMMs run on the 5th-generation
+// tensor cores (tcgen05.mma, BF16 operands from shared memory, FP32 accumulator in
+// tensor memory); master weights, Adam moments, activations' pre-images and
+// gradients are FP32.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -22,82 +23,176 @@
 
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+// ---------------------------------------------------------------- GEMM on the 5th-generation tensor cores
+// C[M x N] = A[M x K] * B[N x K]^T (+ bias[N]); A, B BF16 row-major (K contiguous), C FP32; M, N, K multiples of 64.
+// One CTA of 128 threads per 128 x 64 tile of C. The FP32 accumulator lives in tensor memory (64 columns, lane i =
+// row i of the tile). K runs in groups of up to four 64-wide stages: the threads copy every stage's A and B tiles
+// to shared memory at once (cp.async, 16 bytes each) in the K-major canonical layout without swizzle (8-row x
+// 16-byte core matrices; the two 16-byte K chunks of one instruction 128 B apart, consecutive 8-row groups 1024 B
+// apart), then one thread issues four tcgen05.mma (M 128, N 64, K 16, BF16 in, FP32 accumulate) per stage and
+// tcgen05.commit arrives on an mbarrier when they are done; every wait is bounded. Rows of a last 64-row tile
+// (M = 64 mod 128) are zero in A and not stored. The epilogue reads the accumulator with tcgen05.ld (warp w owns
+// lanes 32w..32w+31), adds the bias and stores FP32 rows.
+constexpr int GM = 128, GN = 64, GK = 64, GSTAGES = 4;
+constexpr int kStageBytes = (GM + GN) * GK * 2;               // A 16 KiB + B 8 KiB
+constexpr int kGemmSmem = GSTAGES * kStageBytes + 64;       // + mbarrier and TMEM slot: 96 KiB, at most two CTAs
+                                                            // (128 of the 512 TMEM columns) per SM
+// instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(GN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
 
-// C[M x N] = A[M x K] * B[N x K]^T (+ bias[N]); A, B BF16 row-major; C FP32.
-// M, N multiples of 64; K multiple of 32. 128 threads: 2 x 2 warps of 32 x 32.
-__global__ void __launch_bounds__(128) k_gemm_bt(const __nv_bfloat16 *__restrict__ A,
-                                                 const __nv_bfloat16 *__restrict__ B, float *__restrict__ C,
-                                                 const float *__restrict__ bias, int M, int N, int K)
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address >> 4 (bits 0-13), leading byte offset >> 4 (16-29) = the K-chunk
+// stride 128 B, stride byte offset >> 4 (32-45) = the 8-row group stride 1024 B, descriptor version 1 (46-47),
+// no swizzle (61-63 = 0)
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr)
 {
-    __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PAD];
-    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PAD];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-    const int gid = lane >> 2, tig = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
 
-    for (int k0 = 0; k0 < K; k0 += TK) {
-        // 64 x 32 bf16 tile = 256 chunks of 8 elements (16 bytes); 2 per thread and operand
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int chunk = t + c * 128;
-            const int row = chunk >> 2, col = (chunk & 3) * 8;
-            *reinterpret_cast<uint4 *>(&As[row][col]) =
-                *reinterpret_cast<const uint4 *>(A + (size_t)(m0 + row) * K + k0 + col);
-            *reinterpret_cast<uint4 *>(&Bs[row][col]) =
-                *reinterpret_cast<const uint4 *>(B + (size_t)(n0 + row) * K + k0 + col);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < TK; kk += 16) {
-            uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r = wm + i * 16 + gid;
-                af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + tig * 2]);
-                af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + tig * 2]);
-                af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + tig * 2 + 8]);
-                af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + tig * 2 + 8]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int n = wn + j * 8 + gid;
-                bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[n][kk + tig * 2]);
-                bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[n][kk + tig * 2 + 8]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                        : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]),
-                          "r"(bfr[j][1]));
-        }
-        __syncthreads();
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, unsigned long long limit_ns)
+{
+    if (mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    while (!mbar_test(bar, parity))
+        if (now_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, const __nv_bfloat16 *__restrict__ B,
+                                                 float *__restrict__ C, const float *__restrict__ bias, int M, int N,
+                                                 int K, int *err, unsigned long long limit_ns)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    // stage g: A tile (128 rows x 64 K) at g * kStageBytes, B tile (64 rows x 64 K) 16 KiB after it
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + GSTAGES * kStageBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + GSTAGES * kStageBytes + 8);
+    const int t = threadIdx.x, warp = t >> 5;
+    const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(saddr(tslot)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = m0 + wm + i * 16 + gid;
-            const int c = n0 + wn + j * 8 + tig * 2;
-            const float b0 = bias ? bias[c] : 0.0f, b1 = bias ? bias[c + 1] : 0.0f;
-            C[(size_t)r * N + c] = acc[i][j][0] + b0;
-            C[(size_t)r * N + c + 1] = acc[i][j][1] + b1;
-            C[(size_t)(r + 8) * N + c] = acc[i][j][2] + b0;
-            C[(size_t)(r + 8) * N + c + 1] = acc[i][j][3] + b1;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+
+    uint32_t parity = 0;
+    bool failed = false;
+    for (int kg = 0; kg < K; kg += GSTAGES * GK) {
+        const int stages = min(GSTAGES, (K - kg) / GK);
+        // chunk c (16 bytes = 8 K values) of a tile sits at byte 16 c: 8-row group c / 64, K chunk (c / 8) % 8,
+        // row c % 8; A rows past M are zero-filled (source size 0)
+        for (int g = 0; g < stages; ++g) {
+            const int k0 = kg + g * GK;
+            unsigned char *As = sm + g * kStageBytes, *Bs = As + GM * GK * 2;
+            for (int c = t; c < GM * 8; c += 128) {
+                const int row = (c >> 6) * 8 + (c & 7), kc = (c >> 3) & 7;
+                const bool in = m0 + row < M;
+                const __nv_bfloat16 *src = A + (size_t)(in ? m0 + row : 0) * K + k0 + kc * 8;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(As + 16 * c)), "l"(src),
+                             "r"(in ? 16 : 0)
+                             : "memory");
+            }
+            for (int c = t; c < GN * 8; c += 128) {
+                const int row = (c >> 6) * 8 + (c & 7), kc = (c >> 3) & 7;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(Bs + 16 * c)),
+                             "l"(B + (size_t)(n0 + row) * K + k0 + kc * 8)
+                             : "memory");
+            }
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the tiles, visible to the tensor core
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int g = 0; g < stages; ++g) {
+                const uint32_t as = saddr(sm + g * kStageBytes), bs = as + GM * GK * 2;
+#pragma unroll
+                for (int kk = 0; kk < GK / 16; ++kk) {
+                    const uint64_t ad = kmajor_desc(as + 256 * kk), bd = kmajor_desc(bs + 256 * kk);
+                    const uint32_t accumulate = (kg > 0 || g > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                 ::"r"(tmem), "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate)
+                                 : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(saddr(bar)) : "memory");
+        }
+        // the group's MMAs read the tiles: every thread waits for them before the next group overwrites them
+        const bool ok = mbar_wait_bounded(saddr(bar), parity, limit_ns);
+        parity ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+    }
+    if (failed) {
+        // a commit that never arrived: report it, give the MMAs once more the limit, free the columns
+        if (t == 0) atomicExch(err, 1);
+        mbar_wait_bounded(saddr(bar), parity ^ 1u, limit_ns);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
+        return;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = m0 + warp * 32 + (t & 31);
+#pragma unroll
+    for (int cb = 0; cb < GN; cb += 16) {
+        uint32_t r[16];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                     "%13, %14, %15}, [%16];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                       "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                       "=r"(r[15])
+                     : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < M) {
+            float4 *dst = reinterpret_cast<float4 *>(C + (size_t)row * N + n0 + cb);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 o = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                       __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+                if (bias) {
+                    const float4 b = *reinterpret_cast<const float4 *>(bias + n0 + cb + 4 * q);
+                    o.x += b.x; o.y += b.y; o.z += b.z; o.w += b.w;
+                }
+                dst[q] = o;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
 }
 
 // y = tanh(z) (or z on the output layer) as BF16 for the next GEMM, FP32 copy kept
@@ -195,6 +290,7 @@ struct bec_mlp {
     float *dy = nullptr, *dz = nullptr, *loss = nullptr;
     __nv_bfloat16 *tA = nullptr, *tB = nullptr;
     int *idx = nullptr;
+    int *d_err = nullptr;            // set by a GEMM whose tensor-core commit never arrived
     float *xin = nullptr, *tgt = nullptr;
     long long adam_t = 0;
     cudaStream_t s = nullptr;
@@ -237,6 +333,37 @@ bec_status mlp_reserve(bec_mlp *m, int batch)
     return BEC_OK;
 }
 
+// C[M x N] = A[M x K] B[N x K]^T (+ bias) on m's stream
+void gemm_bt(bec_mlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *C, const float *bias, int M, int N,
+             int K)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        attr = true;
+    }
+    dim3 grid(N / GN, (M + GM - 1) / GM);
+    k_gemm_tc<<<grid, 128, kGemmSmem, m->s>>>(A, B, C, bias, M, N, K, m->d_err, 2000000000ull);
+    g_launches++;
+}
+
+// BEC_ERR_CUDA when a GEMM since the last check gave up waiting for its tensor-core work (synchronises the stream)
+bec_status check_gemm(bec_mlp *m)
+{
+    int e = 0;
+    if (cudaMemcpyAsync(&e, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, m->s) != cudaSuccess ||
+        cudaStreamSynchronize(m->s) != cudaSuccess) {
+        m->err = cudaGetErrorString(cudaGetLastError());
+        return BEC_ERR_CUDA;
+    }
+    if (e) {
+        cudaMemsetAsync(m->d_err, 0, sizeof(int), m->s);
+        m->err = "MLP GEMM: a tensor-core commit wait gave up";
+        return BEC_ERR_CUDA;
+    }
+    return BEC_OK;
+}
+
 // forward on the first `rows` (multiple of 64) rows of y[0] (FP32 inputs, padded)
 void mlp_forward_dev(bec_mlp *m, int rows)
 {
@@ -244,12 +371,11 @@ void mlp_forward_dev(bec_mlp *m, int rows)
     k_cast_t<<<grid_for((size_t)rows * m->w[0]), 256, 0, s>>>(m->y[0], m->xbf[0], rows, m->w[0], 0);
     for (int l = 0; l < m->L; ++l) {
         const int in = m->w[l], out = m->w[l + 1];
-        dim3 grid(out / TN, rows / TM);
-        k_gemm_bt<<<grid, 128, 0, s>>>(m->xbf[l], m->pbf + m->woff[l], m->z[l + 1], m->p + m->boff[l], rows, out, in);
+        gemm_bt(m, m->xbf[l], m->pbf + m->woff[l], m->z[l + 1], m->p + m->boff[l], rows, out, in);
         const int linear = (l == m->L - 1);
         k_act<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->z[l + 1], m->y[l + 1], m->xbf[l + 1],
                                                            (size_t)rows * out, linear);
-        g_launches += 2;
+        g_launches++;
     }
     g_launches++;
 }
@@ -270,18 +396,14 @@ void mlp_backward_dev(bec_mlp *m, int rows, int valid)
         // dW [out x in] = dZ^T [out x rows] * (X^T [in x rows])^T
         k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 1);
         k_cast_t<<<grid_for((size_t)rows * in), 256, 0, s>>>(m->y[l], m->tB, rows, in, 1);
-        {
-            dim3 grid(in / TN, out / TM);
-            k_gemm_bt<<<grid, 128, 0, s>>>(m->tA, m->tB, m->g + m->woff[l], nullptr, out, in, rows);
-        }
-        g_launches += 5;
+        gemm_bt(m, m->tA, m->tB, m->g + m->woff[l], nullptr, out, in, rows);
+        g_launches += 4;
         if (l > 0) {
             // dX [rows x in] = dZ [rows x out] * W [out x in] = dZ * (W^T [in x out])^T
             k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 0);
             k_cast_t<<<grid_for((size_t)out * in), 256, 0, s>>>(m->p + m->woff[l], m->wt, out, in, 1);
-            dim3 grid(in / TN, rows / TM);
-            k_gemm_bt<<<grid, 128, 0, s>>>(m->tA, m->wt, m->dy, nullptr, rows, in, out);
-            g_launches += 3;
+            gemm_bt(m, m->tA, m->wt, m->dy, nullptr, rows, in, out);
+            g_launches += 2;
         }
     }
 }
@@ -342,6 +464,8 @@ bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed
     for (int v : m->w) maxw = std::max(maxw, v);
     if ((st = mlp_alloc(m, (void **)&m->wt, sizeof(__nv_bfloat16) * maxw * maxw))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->loss, sizeof(float)))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->d_err, sizeof(int)))) return bail(st);
+    if (cudaMemsetAsync(m->d_err, 0, sizeof(int), m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);
     // Glorot-uniform weights on the real block, zero padding and biases
     std::vector<float> h(m->n_params, 0.0f);
     std::mt19937_64 rng(seed);
@@ -420,7 +544,7 @@ bec_status bec_mlp_forward(bec_mlp *m, const float *x, int32_t batch, float *y)
     std::vector<float> h((size_t)rows * ow);
     if (cudaMemcpyAsync(h.data(), m->y[m->L], sizeof(float) * h.size(), cudaMemcpyDeviceToHost, m->s) != cudaSuccess)
         return BEC_ERR_CUDA;
-    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    if ((st = check_gemm(m))) return st;
     for (int r = 0; r < batch; ++r)
         for (int c = 0; c < m->w_real[m->L]; ++c) y[(size_t)r * m->w_real[m->L] + c] = h[(size_t)r * ow + c];
     return BEC_OK;
@@ -446,7 +570,7 @@ bec_status bec_mlp_gradients(bec_mlp *m, const float *x, const float *target, in
     cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->s);
     std::vector<float> h(m->n_params);
     cudaMemcpyAsync(h.data(), m->g, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, m->s);
-    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    if ((st = check_gemm(m))) return st;
     if (loss) *loss = l;
     if (grads) {
         size_t k = 0;
@@ -524,7 +648,7 @@ bec_status bec_mlp_train(bec_mlp *m, const float *x, const float *target, int32_
     }
     std::vector<float> hist(steps, 0.0f);
     if (steps > 0) cudaMemcpyAsync(hist.data(), dhist, sizeof(float) * steps, cudaMemcpyDeviceToHost, m->s);
-    if (cudaStreamSynchronize(m->s) != cudaSuccess) return BEC_ERR_CUDA;
+    if ((st = check_gemm(m))) return st;
     if (loss_history)
         for (int s = 0; s < steps; ++s) loss_history[s] = hist[s];
     return cudaGetLastError() == cudaSuccess ? BEC_OK : BEC_ERR_CUDA;
