@@ -91,7 +91,8 @@ struct bec_ctx {
     int plan_mode = -2;                  // -2: not chosen yet, else the schedule candidate (ensure_plan)
     int plane_occupancy = 0;             // per-pass plane launches: 0 = 16 warps per SM, 1 = 20
     bool pencil_tuned = false;           // per-pass pencil launches: each class's own pencil kernel (pencil_kind)
-    int *d_pflags = nullptr;             // batched: [0] error flag of the TMA pencil pass, [1] a flag nothing sets
+    int *d_pflags = nullptr;             // batched: [0] error flag of the TMA pencil pass, [1] a flag nothing sets,
+                                         // [2] CTAs finished in the plane launch that advances the step index
     std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // kGraphSteps steps, 1 step
     long long graph_kernels[2] = {0, 0};                  // kernels per replay of each
@@ -426,22 +427,43 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
 }
 
 // put_step: write ctx->step into the device step scalar first (eager launches; a captured step graph
-// leaves it to the step before); skip_fused: leave out the classes of the fused step plan
+// leaves it to the step before); skip_fused: leave out the classes of the fused step plan. advanced != NULL:
+// the step index is advanced in the same pass where a class can carry it -- the register-path plane launch
+// with the fewest CTAs (at most kMaxCarrierCtas, one atomic each) runs last and its last CTA increments the
+// index -- and *advanced tells the caller whether that happened.
+constexpr int kMaxCarrierCtas = 16384;
+
 bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr, bool put_step = true,
-                             bool skip_fused = false)
+                             bool skip_fused = false, bool *advanced = nullptr)
 {
     if (put_step) {
         fp32_put_step(ctx->d_step, (uint32_t)ctx->step, ctx->stream);
         CKL();
     }
-    for (auto &c : ctx->classes) {
-        if (c.geom.n_traj == 0) continue;
-        if (skip_fused && ctx->fused[&c - &ctx->classes[0]]) continue;
-        const size_t ci = &c - &ctx->classes[0];
+    const int nc = (int)ctx->classes.size();
+    auto launched = [&](int ci) {
+        const ClassRec &c = ctx->classes[ci];
+        return c.geom.n_traj > 0 && !(skip_fused && ctx->fused[ci]);
+    };
+    auto fast = [&](int ci) { return ctx->use_fast && fp32_fast_plane_supported(ctx->classes[ci].geom); };
+    int carrier = -1;
+    if (advanced) {
+        for (int ci = 0; ci < nc; ++ci)
+            if (launched(ci) && fast(ci) && fp32_plane_fast_ctas(ctx->classes[ci].geom) <= kMaxCarrierCtas &&
+                (carrier < 0 ||
+                 fp32_plane_fast_ctas(ctx->classes[ci].geom) < fp32_plane_fast_ctas(ctx->classes[carrier].geom)))
+                carrier = ci;
+        *advanced = carrier >= 0;
+    }
+    for (int k = 0; k < nc; ++k) {
+        // the carrier, if any, goes last
+        const int ci = carrier < 0 ? k : (k < carrier ? k : k + 1 < nc ? k + 1 : carrier);
+        if (!launched(ci)) continue;
+        ClassRec &c = ctx->classes[ci];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
-        if (ctx->use_fast && fp32_fast_plane_supported(c.geom)) {
+        if (fast(ci)) {
             fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step, ctx->plane_occupancy,
-                            ctx->stream);
+                            ci == carrier ? ctx->d_pflags + 2 : nullptr, ctx->stream);
         } else {
             float2 *tx, *ty;
             bec_status st;
@@ -473,9 +495,10 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
         for (int i = 0; i < 4; ++i) mf[i] = make_float2((float)ctx->pulse[i].x, (float)ctx->pulse[i].y);
     bec_status st;
     if ((st = batched_zpass_all(ctx, pre, 0.5f, false, nullptr, false, nullptr, fused))) return st;
-    if ((st = batched_ppass_all(ctx, nullptr, false, fused))) return st;
+    bool advanced = false;
+    if ((st = batched_ppass_all(ctx, nullptr, false, fused, fused ? nullptr : &advanced))) return st;
     if (fused) step_launch(ctx->plan, ctx->d_gparams, ctx->d_step, pre + 0.5f, has_m ? mf : nullptr, ctx->stream);
-    else fp32_inc_step(ctx->d_step, ctx->stream);
+    else if (!advanced) fp32_inc_step(ctx->d_step, ctx->stream);
     CKL();
     return BEC_OK;
 }
@@ -1140,8 +1163,8 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
         CKA(dalloc(ctx, &ctx->d_gparams, (size_t)ng));
         CKA(cudaMemcpyAsync(ctx->d_gparams, gfs.data(), sizeof(GroupParamsF) * ng, cudaMemcpyHostToDevice, ctx->stream));
         CKA(dalloc(ctx, &ctx->d_step, (size_t)1));
-        CKA(dalloc(ctx, &ctx->d_pflags, (size_t)2));
-        CKA(cudaMemsetAsync(ctx->d_pflags, 0, 2 * sizeof(int), ctx->stream));
+        CKA(dalloc(ctx, &ctx->d_pflags, (size_t)4));
+        CKA(cudaMemsetAsync(ctx->d_pflags, 0, 4 * sizeof(int), ctx->stream));
         {
             const char *g = std::getenv("BEC_CUDA_GRAPHS");
             ctx->use_graphs = !(g && g[0] == '0');

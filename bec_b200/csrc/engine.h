@@ -184,7 +184,9 @@ bool fp32_fast_plane_supported(const ClassGeom &c);
 bool fp32_fast_pencil_supported(const ClassGeom &c);
 // occupancy: 0 = 16 warps per SM, no spill; 1 = 20 warps per SM at 96 registers (an autotuner choice)
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     const uint32_t *d_step, int occupancy, cudaStream_t s);
+                     uint32_t *d_step, int occupancy, int *inc_done, cudaStream_t s);
+// CTAs of that launch; inc_done != NULL: its last CTA also advances *d_step (inc_done: a zero int counter)
+int fp32_plane_fast_ctas(const ClassGeom &c);
 // tw_full: nz entries W_nz^e; frac: kick in units of dt; scale: 1/cells times out_scale;
 // m: optional pulse matrix (row-major, 4 entries) or NULL; obs: when not NULL the pass
 // ends a step and writes per-z partial moments [traj][tile][z][4] (tiles = fp32_fast_pencil_tiles)

@@ -15,14 +15,30 @@ using stepk::PencilArgs;
 using stepk::VBlock;
 
 // ---------------------------------------------------------------- plane pass, N = 8, 16
+// done != NULL: this launch also advances the Philox step index *stepp once every CTA has finished (every CTA
+// read it at its start): the CTA that finishes last (the atomic counter reaches the grid size) resets the counter
+// and increments the index, which the next step's kernels read. The one-thread increment launch is then not needed.
+__device__ __forceinline__ void advance_step_if_last(uint32_t *stepp, int *done)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1) == (int)gridDim.x - 1) {
+            *done = 0;
+            atomicAdd(stepp, 1u);
+        }
+    }
+}
+
 template <int N, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_plane(float4 *__restrict__ state, int nz, int cells,
                                                const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
-                                               const int *__restrict__ tlocal, const uint32_t *__restrict__ stepp)
+                                               const int *__restrict__ tlocal, uint32_t *stepp, int *done)
 {
     extern __shared__ float4 tile[];   // 4 warps x W planes x N^2
     stepk::plane_body<N>(VBlock{(int)threadIdx.x, (int)blockIdx.x, 0, 128}, state, nz, cells, gp, tgroup, tlocal,
                          *stepp, tile);
+    if (done) advance_step_if_last(stepp, done);
 }
 
 // ---------------------------------------------------------------- plane pass, 32 x 32, two warps a plane
@@ -30,12 +46,13 @@ template <int MINB>
 __global__ void __launch_bounds__(64, MINB) k_plane32s(float4 *__restrict__ state, int nz, int cells,
                                                       const GroupParamsF *__restrict__ gp,
                                                       const int *__restrict__ tgroup, const int *__restrict__ tlocal,
-                                                      const uint32_t *__restrict__ stepp)
+                                                      uint32_t *stepp, int *done)
 {
     __shared__ float4 tile[1024];
     __shared__ float4 xb[512];
     stepk::plane32_body(VBlock{(int)threadIdx.x, (int)blockIdx.x, 0, 64}, state, nz, cells, gp, tgroup, tlocal,
                         *stepp, tile, xb);
+    if (done) advance_step_if_last(stepp, done);
 }
 
 // ---------------------------------------------------------------- pencil pass
@@ -90,7 +107,7 @@ void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, co
 
 template <int N, int MINB>
 void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                  const uint32_t *step, cudaStream_t s)
+                  uint32_t *step, int *done, cudaStream_t s)
 {
     constexpr int W = 32 / N;
     const int planes = c.n_traj * c.nz;
@@ -100,15 +117,15 @@ void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, con
         cudaFuncSetAttribute(k_plane<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_plane<N, MINB><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
+    k_plane<N, MINB><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step, done);
     g_launches++;
 }
 
 template <int MINB>
 void launch_plane32s(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     const uint32_t *step, cudaStream_t s)
+                     uint32_t *step, int *done, cudaStream_t s)
 {
-    k_plane32s<MINB><<<c.n_traj * c.nz, 64, 0, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step);
+    k_plane32s<MINB><<<c.n_traj * c.nz, 64, 0, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step, done);
     g_launches++;
 }
 
@@ -126,24 +143,29 @@ bool fp32_fast_pencil_supported(const ClassGeom &c)
     return (c.nz == 64 || c.nz == 128 || c.nz == 256) && (c.nx * c.ny) % 16 == 0 && c.nx * c.ny >= 16;
 }
 
+int fp32_plane_fast_ctas(const ClassGeom &c)
+{
+    return c.nx == 32 ? c.n_traj * c.nz : c.n_traj * c.nz / (4 * (32 / c.nx));
+}
+
 void fp32_plane_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
-                     const uint32_t *step, int occupancy, cudaStream_t s)
+                     uint32_t *step, int occupancy, int *inc_done, cudaStream_t s)
 {
     if (c.n_traj <= 0) return;
     // occupancy 0: 16 warps per SM (8x8 / 16x16: 4 CTAs of 128 threads; 32x32: 8 CTAs of 64), no register spill;
     // occupancy 1: 20 warps per SM (5 and 10 CTAs), 96 registers with a small spill
     switch (c.nx) {
     case 8:
-        if (occupancy) launch_plane<8, 5>(state, c, gp, tgroup, tlocal, step, s);
-        else launch_plane<8, 4>(state, c, gp, tgroup, tlocal, step, s);
+        if (occupancy) launch_plane<8, 5>(state, c, gp, tgroup, tlocal, step, inc_done, s);
+        else launch_plane<8, 4>(state, c, gp, tgroup, tlocal, step, inc_done, s);
         break;
     case 16:
-        if (occupancy) launch_plane<16, 5>(state, c, gp, tgroup, tlocal, step, s);
-        else launch_plane<16, 4>(state, c, gp, tgroup, tlocal, step, s);
+        if (occupancy) launch_plane<16, 5>(state, c, gp, tgroup, tlocal, step, inc_done, s);
+        else launch_plane<16, 4>(state, c, gp, tgroup, tlocal, step, inc_done, s);
         break;
     case 32:
-        if (occupancy) launch_plane32s<10>(state, c, gp, tgroup, tlocal, step, s);
-        else launch_plane32s<8>(state, c, gp, tgroup, tlocal, step, s);
+        if (occupancy) launch_plane32s<10>(state, c, gp, tgroup, tlocal, step, inc_done, s);
+        else launch_plane32s<8>(state, c, gp, tgroup, tlocal, step, inc_done, s);
         break;
     default: break;
     }
