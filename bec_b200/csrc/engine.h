@@ -178,6 +178,9 @@ void render_colour(const float *level, int n, float max_level, float4 *rgba, cud
 
 // launch counter (kernels this library enqueued since the counter was reset)
 extern thread_local long long g_launches;
+// Sets the kernel's dynamic shared memory limit to `bytes` on the current device, once per (kernel, device);
+// safe from several host threads (a process may drive several GPUs).
+cudaError_t ensure_smem_limit(const void *kernel, int bytes);
 
 // fused_passes.cu: register-resident passes (square planes 8/16/32; nz = 64/128/256)
 bool fp32_fast_plane_supported(const ClassGeom &c);

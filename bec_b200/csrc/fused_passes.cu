@@ -95,11 +95,7 @@ void launch_pencil(float4 *state, const ClassGeom &c, const GroupParamsF *gp, co
 {
     const int tiles = c.nx * c.ny / 16;
     const size_t smem = stepk::pencil_smem_bytes<NZ>();
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_pencil<NZ, OBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    ensure_smem_limit((const void *)k_pencil<NZ, OBS>, (int)smem);
     k_pencil<NZ, OBS><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, tgroup, tw,
                                                          pa, obs, inv_out_scale, kin);
     g_launches++;
@@ -112,11 +108,7 @@ void launch_plane(float4 *state, const ClassGeom &c, const GroupParamsF *gp, con
     constexpr int W = 32 / N;
     const int planes = c.n_traj * c.nz;
     const size_t smem = sizeof(float4) * 4 * W * N * N;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_plane<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    ensure_smem_limit((const void *)k_plane<N, MINB>, (int)smem);
     k_plane<N, MINB><<<planes / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, tgroup, tlocal, step, done);
     g_launches++;
 }

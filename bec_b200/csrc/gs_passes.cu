@@ -300,11 +300,7 @@ void launch_gs_plane(float2 *state, const ClassGeom &c, const GroupParamsF *gp, 
 {
     constexpr int W = 32 / N;
     const size_t smem = sizeof(float2) * 4 * W * N * N;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gs_plane<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    ensure_smem_limit((const void *)k_gs_plane<N, MODE>, (int)smem);
     k_gs_plane<N, MODE><<<c.n_traj * c.nz / (4 * W), 128, smem, s>>>(state, c.nz, c.cells, gp, gs, tgroup, norm_in,
                                                                       norm_clear, out, xsums, in_scale, active);
     g_launches++;
@@ -317,11 +313,7 @@ void launch_gs_pencil(float2 *state, const ClassGeom &c, const GroupParamsF *gp,
 {
     const int tiles = c.nx * c.ny / 16;
     const size_t smem = sizeof(float2) * (16 * NZ + NZ) + sizeof(float) * (3 * NZ + 3 * 16);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gs_pencil<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    ensure_smem_limit((const void *)k_gs_pencil<NZ>, (int)smem);
     k_gs_pencil<NZ><<<c.n_traj * tiles, NZ, smem, s>>>(state, c.nx, c.lx, c.ny, c.cells, tiles, gp, gs, tgroup, tw,
                                                        a, norm, ekin, active);
     g_launches++;

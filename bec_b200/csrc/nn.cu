@@ -11,6 +11,7 @@
 // tensor memory); master weights, Adam moments, activations' pre-images and
 // gradients are FP32.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -79,9 +80,21 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
     return true;
 }
 
+// a wait for a flag that nothing sets (fault injection): false after limit_ns
+__device__ __noinline__ bool wait_flag(const int *flag, unsigned long long limit_ns)
+{
+    const unsigned long long t0 = now_ns();
+    while (*(volatile const int *)flag == 0) {
+        __nanosleep(1000);
+        if (now_ns() - t0 > limit_ns) return false;
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, const __nv_bfloat16 *__restrict__ B,
                                                  float *__restrict__ C, const float *__restrict__ bias, int M, int N,
-                                                 int K, int *err, unsigned long long limit_ns)
+                                                 int K, int *err, const int *never, int stall,
+                                                 unsigned long long limit_ns)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     // stage g: A tile (128 rows x 64 K) at g * kStageBytes, B tile (64 rows x 64 K) 16 KiB after it
@@ -147,18 +160,20 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          ::"r"(saddr(bar)) : "memory");
         }
-        // the group's MMAs read the tiles: every thread waits for them before the next group overwrites them
-        const bool ok = mbar_wait_bounded(saddr(bar), parity, limit_ns);
-        parity ^= 1u;
+        // the group's MMAs read the tiles: every thread waits for them before the next group overwrites them;
+        // stall (fault injection): the first group also waits for a flag that nothing sets
+        bool ok = mbar_wait_bounded(saddr(bar), parity, limit_ns);
+        if (stall && kg == 0 && ok) ok = wait_flag(never, limit_ns);
         if (__syncthreads_or(!ok)) {
             failed = true;
             break;
         }
+        parity ^= 1u;
     }
     if (failed) {
-        // a commit that never arrived: report it, give the MMAs once more the limit, free the columns
+        // a wait that ran out: report it, give the group's MMAs once more the limit, free the columns
         if (t == 0) atomicExch(err, 1);
-        mbar_wait_bounded(saddr(bar), parity ^ 1u, limit_ns);
+        mbar_wait_bounded(saddr(bar), parity, limit_ns);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
@@ -290,7 +305,7 @@ struct bec_mlp {
     float *dy = nullptr, *dz = nullptr, *loss = nullptr;
     __nv_bfloat16 *tA = nullptr, *tB = nullptr;
     int *idx = nullptr;
-    int *d_err = nullptr;            // set by a GEMM whose tensor-core commit never arrived
+    int *d_err = nullptr;            // [0] set by a GEMM whose wait ran out, [1] a flag nothing sets
     float *xin = nullptr, *tgt = nullptr;
     long long adam_t = 0;
     cudaStream_t s = nullptr;
@@ -337,17 +352,19 @@ bec_status mlp_reserve(bec_mlp *m, int batch)
 void gemm_bt(bec_mlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *C, const float *bias, int M, int N,
              int K)
 {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-        attr = true;
-    }
+    ensure_smem_limit((const void *)k_gemm_tc, kGemmSmem);
+    // BEC_STEP_WAIT_LIMIT_MS bounds the device-side waits (2 s by default); BEC_GEMM_INJECT_STALL=1 makes the
+    // first K group of every CTA also wait for a flag that nothing sets (the error path, without a fault)
+    unsigned long long limit_ns = 2000000000ull;
+    if (const char *v = std::getenv("BEC_STEP_WAIT_LIMIT_MS")) limit_ns = 1000000ull * std::strtoull(v, nullptr, 10);
+    const char *inj = std::getenv("BEC_GEMM_INJECT_STALL");
+    const int stall = inj && std::atoi(inj) ? 1 : 0;
     dim3 grid(N / GN, (M + GM - 1) / GM);
-    k_gemm_tc<<<grid, 128, kGemmSmem, m->s>>>(A, B, C, bias, M, N, K, m->d_err, 2000000000ull);
+    k_gemm_tc<<<grid, 128, kGemmSmem, m->s>>>(A, B, C, bias, M, N, K, m->d_err, m->d_err + 1, stall, limit_ns);
     g_launches++;
 }
 
-// BEC_ERR_CUDA when a GEMM since the last check gave up waiting for its tensor-core work (synchronises the stream)
+// BEC_ERR_CUDA when a GEMM since the last check gave up a wait (synchronises the stream)
 bec_status check_gemm(bec_mlp *m)
 {
     int e = 0;
@@ -358,7 +375,7 @@ bec_status check_gemm(bec_mlp *m)
     }
     if (e) {
         cudaMemsetAsync(m->d_err, 0, sizeof(int), m->s);
-        m->err = "MLP GEMM: a tensor-core commit wait gave up";
+        m->err = "MLP GEMM: a tensor-core wait gave up";
         return BEC_ERR_CUDA;
     }
     return BEC_OK;
@@ -464,8 +481,8 @@ bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed
     for (int v : m->w) maxw = std::max(maxw, v);
     if ((st = mlp_alloc(m, (void **)&m->wt, sizeof(__nv_bfloat16) * maxw * maxw))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->loss, sizeof(float)))) return bail(st);
-    if ((st = mlp_alloc(m, (void **)&m->d_err, sizeof(int)))) return bail(st);
-    if (cudaMemsetAsync(m->d_err, 0, sizeof(int), m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);
+    if ((st = mlp_alloc(m, (void **)&m->d_err, 2 * sizeof(int)))) return bail(st);
+    if (cudaMemsetAsync(m->d_err, 0, 2 * sizeof(int), m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);
     // Glorot-uniform weights on the real block, zero padding and biases
     std::vector<float> h(m->n_params, 0.0f);
     std::mt19937_64 rng(seed);

@@ -235,19 +235,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
 
 EncodeTiledFn encode_fn()
 {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // looked up once per process (a thread-safe static initialisation)
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
                 cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-        else
-            cudaGetLastError();
-    }
+            return reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -279,17 +277,14 @@ cudaError_t launch_tma(float4 *state, const ClassGeom &c, const TmaArgs &A0, cud
         CUDA_SUCCESS)
         return cudaErrorInvalidValue;
     constexpr size_t smem = tma_smem_bytes<NZ>();
-    static int grid_max = 0;
     cudaError_t e;
-    if (!grid_max) {
-        int dev = 0, sms = 0, per_sm = 0;
-        if ((e = cudaFuncSetAttribute(k_pencil_tma<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-        if ((e = cudaGetDevice(&dev))) return e;
-        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pencil_tma<NZ>, kThreads, smem))) return e;
-        if (per_sm < 1) return cudaErrorInvalidConfiguration;
-        grid_max = sms * per_sm;
-    }
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = ensure_smem_limit((const void *)k_pencil_tma<NZ>, (int)smem))) return e;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pencil_tma<NZ>, kThreads, smem))) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int grid_max = sms * per_sm;
     TmaArgs A = A0;
     A.plane = plane;
     A.tiles_per_traj = plane / PEN;

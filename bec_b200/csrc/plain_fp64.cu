@@ -7,11 +7,29 @@
 // ~1e-12 relative) and the baseline that the batched FP32 path is measured
 // against. FFT axes use this library's shared-memory radix-2 stages
 // (fft_smem.cuh) in place of cuFFT + transposes (batchfft.cu:130-180).
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "engine.h"
 #include "fft_smem.cuh"
 #include "reduce.cuh"
 
 thread_local long long g_launches = 0;
+
+cudaError_t ensure_smem_limit(const void *kernel, int bytes)
+{
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({kernel, dev})) return cudaSuccess;
+    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    done.insert({kernel, dev});
+    return cudaSuccess;
+}
 
 namespace {
 

@@ -84,3 +84,27 @@ def test_gpu_training_reduces_loss():
     assert hist[-20:].mean() < 0.1 * hist[:5].mean()
     loss, _ = net.gradients(x, t)
     assert loss < 0.1 * hist[:5].mean()
+
+
+@pytest.mark.gpu
+def test_gemm_wait_that_runs_out_is_reported(monkeypatch):
+    """A tensor-core GEMM whose wait runs out (its first K group also waits for a flag that nothing sets, with a
+    20 ms limit) ends with BEC_ERR_CUDA after its MMAs have finished and its tensor memory is freed; the device
+    stays usable and the next call computes the same bits as a fresh network."""
+    from bec_b200._abi import BEC_ERR_CUDA
+    from bec_b200.engine import MLP, BecError
+    x, _ = _data(100)
+    p = _params(WIDTHS)
+    monkeypatch.setenv("BEC_STEP_WAIT_LIMIT_MS", "20")
+    monkeypatch.setenv("BEC_GEMM_INJECT_STALL", "1")
+    net = MLP(WIDTHS, seed=0)
+    net.set_params(p)
+    with pytest.raises(BecError) as ei:
+        net.forward(x)
+    assert ei.value.status == BEC_ERR_CUDA
+    monkeypatch.delenv("BEC_GEMM_INJECT_STALL")
+    monkeypatch.delenv("BEC_STEP_WAIT_LIMIT_MS")
+    y = net.forward(x)
+    fresh = MLP(WIDTHS, seed=0)
+    fresh.set_params(p)
+    np.testing.assert_array_equal(y, fresh.forward(x))
