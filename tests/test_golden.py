@@ -5,7 +5,7 @@ The stored curve's loss and detuning parameters were never recorded, so it
 pins the physics loosely: with the workload's Rb-87 loss rates the oracle
 follows it within 0.006 to 0.1 s and 0.035 to 0.3 s (first dip and revival).
 The oracle's own curve (generated by tests/golden/make_golden.py) checks the
-batched FP32 engine over all 15000 steps against the FP64 north-star bound of
+batched FP32 engine over all 15000 steps against an FP64-parity bound of
 1e-3 in visibility."""
 import json
 import os

@@ -109,7 +109,7 @@ def test_ensemble_16x16x128_200ms():
     eng, rep, mom, traj, axial = _engine_run(p, meta)
     assert rep.mu == pytest.approx(float(fx["gs_mu"]), rel=1e-10)
     err = _compare("long_ensemble_16x16x128", p, meta, fx, eng, mom, traj, axial)
-    assert err["visibility"] < 2e-4                   # the north-star bound is 1e-3
+    assert err["visibility"] < 2e-4                   # the stated FP32 visibility bound is 1e-3
     assert err["N1"] < 5e-4 and err["N2"] < 5e-4
     assert err["traj_population"] < 5e-4
     assert err["phase"] < 1e-3
