@@ -33,6 +33,27 @@ def test_reference_arm_line():
     assert d["e2e"] == {"value": d["value"], "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
+def test_baseline_samples_keep_the_batch_mix():
+    """The CPU and plain-FP64 baseline samples hold every grid class in the batch's proportion (largest
+    remainders), so their traj-steps/s compare with the batch's."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from bec_b200.configs import uneven_batch
+    groups = uneven_batch(n_traj=1024, seed=2)
+    counts = {}
+    for p in groups:
+        counts[(p.nvx, p.nvy, p.nvz)] = counts.get((p.nvx, p.nvy, p.nvz), 0) + 1
+    for n in (3, 24, 32, 100):
+        s = bench.mix_sample(groups, n)
+        assert len(s) == n and len({id(p) for p in s}) == n
+        got = {}
+        for p in s:
+            got[(p.nvx, p.nvy, p.nvz)] = got.get((p.nvx, p.nvy, p.nvz), 0) + 1
+        for k, c in counts.items():
+            assert abs(got.get(k, 0) - n * c / len(groups)) < 1.0
+    assert bench.mix_sample(groups[:5], 32) == groups[:5]
+
+
 def test_rank_to_physical_gpu(monkeypatch):
     sys.path.insert(0, ROOT)
     import bench
