@@ -480,7 +480,8 @@ bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *
 // One split step of every class, ending with its plane pass: kick fraction pre of dt before this step's half
 // kick (0.5 while the previous step's second half kick is pending), then any pending pulse. The classes of
 // the fused plan run as one launch of the fused step kernel, which advances the device step index; the
-// others launch their own passes, and without a fused plan a one-thread launch advances it. put_step writes
+// others launch their own passes, and without a fused plan the smallest plane launch advances it (or, when
+// no class can carry it, a one-thread launch). put_step writes
 // the host step index to the device first (eager steps); a captured step graph leaves it to the step before.
 bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
 {
@@ -773,7 +774,8 @@ bec_status batched_resolve(bec_ctx *ctx, bool observe)
     return BEC_OK;
 }
 
-// Error flag of the fused step kernel: a dependency wait that gave up (the kernel bounds every wait).
+// Error flags of the fused step kernel (a dependency wait that gave up) and of the TMA pencil kernel (a tile
+// load wait that gave up); both kernels bound every wait.
 bec_status check_step_error(bec_ctx *ctx)
 {
     int err = 0;
@@ -792,9 +794,10 @@ bec_status check_step_error(bec_ctx *ctx)
 
 // ---------------------------------------------------------------- captured step loop
 // A steady step (the previous step's second half-kick pending, no pulse, no observation) launches the
-// same kernels with the same arguments every time: the full kick in the pencil passes, an increment of
-// the device step scalar, the plane passes. kGraphSteps of them, and one, are captured once per context
-// and replayed; the device step scalar is set once before a stretch of replays.
+// same kernels with the same arguments every time: the full kick in the pencil passes, the plane passes
+// (the step scalar advanced by the last CTA of the smallest one, or of the fused kernel, or by a one-thread
+// launch). kGraphSteps of them, and one, are captured once per context and replayed; the device step
+// scalar is set once before a stretch of replays.
 constexpr int kGraphSteps = 8;
 
 bec_status capture_steps(bec_ctx *ctx, int k, cudaGraphExec_t *out, long long *kernels)

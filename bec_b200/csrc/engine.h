@@ -113,7 +113,8 @@ void fp32_zpass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const
 void fp32_ppass(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup,
                 const int *tlocal, const float2 *tw_x, const float2 *tw_y, const uint32_t *d_step, cudaStream_t s);
 // the plane passes read the Philox step index from a device scalar, so a captured step graph can replay:
-// an eagerly launched step writes it (fp32_put_step), a graph step increments it (fp32_inc_step)
+// an eagerly launched step writes it (fp32_put_step); a step advances it at its end (fp32_inc_step, or the
+// last CTA of a plane launch given inc_done, or of the fused step kernel)
 void fp32_put_step(uint32_t *d_step, uint32_t v, cudaStream_t s);
 void fp32_inc_step(uint32_t *d_step, cudaStream_t s);
 int fp32_zpass_tiles(const ClassGeom &c);   // tiles per trajectory of the z pass (obs_partial layout)
