@@ -69,6 +69,8 @@ struct ClassRec {
     float2 *kin_tab[2] = {nullptr, nullptr};   // kinetic phase tables for kick fractions 0.5 and 1 (register pencils)
     int pencil_kind = 0;      // the tuned per-pass schedules' pencil kernel for this class (kPencilRegister ...)
     double pencil_ms[2] = {-1.0, -1.0};        // autotuner: ms per launch of each pencil kernel
+    bool onchip = false;      // the tuned schedules run this class's steady steps as one on-chip launch
+    double plane_ms = -1.0, onchip_ms = -1.0;  // autotuner: its plane launch, its on-chip step
 };
 
 } // namespace
@@ -91,6 +93,7 @@ struct bec_ctx {
     int plan_mode = -2;                  // -2: not chosen yet, else the schedule candidate (ensure_plan)
     int plane_occupancy = 0;             // per-pass plane launches: 0 = 16 warps per SM, 1 = 20
     bool pencil_tuned = false;           // per-pass pencil launches: each class's own pencil kernel (pencil_kind)
+    bool step_onchip = false;            // the step being launched is steady: classes with `onchip` take one launch
     int *d_pflags = nullptr;             // batched: [0] error flag of the TMA pencil pass, [1] a flag nothing sets,
                                          // [2] CTAs finished in the plane launch that advances the step index
     std::string plan_desc;               // the chosen plan and the autotuner's timings (JSON)
@@ -357,6 +360,12 @@ bec_status plain_step(bec_ctx *ctx, GroupRec &gr, int t)
 // ends_step: no plane pass follows, so the pass leaves the state in the form a z pass reads
 // ev (optional): per class (start, stop) events recorded around that class's launch
 // skip_fused: leave out the classes of the fused step plan (their pencil pass runs inside it)
+// a class whose steady step runs as one on-chip launch in the step being launched
+bool onchip_now(const bec_ctx *ctx, const ClassRec &c)
+{
+    return ctx->step_onchip && ctx->pencil_tuned && c.onchip && c.kin_tab[1] && fp32_onchip_supported(c.geom);
+}
+
 bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, const double2 *m2,
                              bool ends_step = false, std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr,
                              bool skip_fused = false)
@@ -389,6 +398,7 @@ bec_status batched_zpass_all(bec_ctx *ctx, float pre, float post, bool observe, 
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
         if (skip_fused && ctx->fused[&c - &ctx->classes[0]]) continue;
+        if (onchip_now(ctx, c)) continue;           // its plane-pass slot runs the whole step
         bec_status st;
         z.scale = (float)(1.0 / (double)c.geom.cells);
         z.out_scale = ends_step ? (float)(c.geom.nx * c.geom.ny) : 1.0f;
@@ -445,13 +455,15 @@ bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *
         const ClassRec &c = ctx->classes[ci];
         return c.geom.n_traj > 0 && !(skip_fused && ctx->fused[ci]);
     };
-    auto fast = [&](int ci) { return ctx->use_fast && fp32_fast_plane_supported(ctx->classes[ci].geom); };
+    auto onchip = [&](int ci) { return onchip_now(ctx, ctx->classes[ci]); };
+    auto fast = [&](int ci) { return onchip(ci) || (ctx->use_fast && fp32_fast_plane_supported(ctx->classes[ci].geom)); };
+    auto ctas = [&](int ci) {
+        return onchip(ci) ? ctx->classes[ci].geom.n_traj : fp32_plane_fast_ctas(ctx->classes[ci].geom);
+    };
     int carrier = -1;
     if (advanced) {
         for (int ci = 0; ci < nc; ++ci)
-            if (launched(ci) && fast(ci) && fp32_plane_fast_ctas(ctx->classes[ci].geom) <= kMaxCarrierCtas &&
-                (carrier < 0 ||
-                 fp32_plane_fast_ctas(ctx->classes[ci].geom) < fp32_plane_fast_ctas(ctx->classes[carrier].geom)))
+            if (launched(ci) && fast(ci) && ctas(ci) <= kMaxCarrierCtas && (carrier < 0 || ctas(ci) < ctas(carrier)))
                 carrier = ci;
         *advanced = carrier >= 0;
     }
@@ -461,7 +473,13 @@ bec_status batched_ppass_all(bec_ctx *ctx, std::pair<cudaEvent_t, cudaEvent_t> *
         if (!launched(ci)) continue;
         ClassRec &c = ctx->classes[ci];
         if (ev) CKC(cudaEventRecord(ev[ci].first, ctx->stream));
-        if (fast(ci)) {
+        if (onchip(ci)) {
+            float2 *twf;
+            bec_status st;
+            if ((st = get_tw32_full(ctx, c.geom.nz, &twf))) return st;
+            fp32_onchip_step(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, twf, c.kin_tab[1], ctx->d_step,
+                             ci == carrier ? ctx->d_pflags + 2 : nullptr, ctx->stream);
+        } else if (fast(ci)) {
             fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step, ctx->plane_occupancy,
                             ci == carrier ? ctx->d_pflags + 2 : nullptr, ctx->stream);
         } else {
@@ -495,6 +513,9 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
     if (has_m)
         for (int i = 0; i < 4; ++i) mf[i] = make_float2((float)ctx->pulse[i].x, (float)ctx->pulse[i].y);
     bec_status st;
+    // a steady step (the previous step's second half kick pending, no pulse): the on-chip classes take one launch
+    ctx->step_onchip = !fused && pre == 0.5f && !has_m;
+    struct Clear { bool &f; ~Clear() { f = false; } } clear{ctx->step_onchip};
     if ((st = batched_zpass_all(ctx, pre, 0.5f, false, nullptr, false, nullptr, fused))) return st;
     bool advanced = false;
     if ((st = batched_ppass_all(ctx, nullptr, false, fused, fused ? nullptr : &advanced))) return st;
@@ -516,7 +537,7 @@ bec_status batched_step(bec_ctx *ctx, float pre, bool put_step)
 constexpr int kPerPassCandidates = 4;
 constexpr int kAllCandidates = kPerPassCandidates + kStepCandidates;
 const char *const kPerPassNames[kPerPassCandidates] = {"unfused", "unfused-20", "unfused-tma", "unfused-20-tma"};
-constexpr size_t kPickClasses = 12;   // classes whose pencil picks the plan cache keeps
+constexpr size_t kPickClasses = 11;   // classes whose picks the plan cache keeps (two bits each above bit 8)
 
 std::string candidate_name(int c)
 {
@@ -537,6 +558,8 @@ bec_status pick_pencil_kernels(bec_ctx *ctx)
     for (auto &c : ctx->classes) {
         c.pencil_kind = kPencilRegister;
         c.pencil_ms[0] = c.pencil_ms[1] = -1.0;
+        c.onchip = false;
+        c.plane_ms = c.onchip_ms = -1.0;
         if (c.geom.n_traj == 0 || !ctx->use_fast || !fp32_fast_pencil_supported(c.geom) || !c.kin_tab[1]) continue;
         float2 *twf;
         bec_status st;
@@ -559,6 +582,27 @@ bec_status pick_pencil_kernels(bec_ctx *ctx)
             CKC(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
             c.pencil_ms[kind] = ms / 3.0;
             if (c.pencil_ms[kind] < c.pencil_ms[c.pencil_kind]) c.pencil_kind = kind;
+        }
+        // an 8x8x64 class: its steady step as one on-chip launch against its faster pencil launch plus its plane
+        // launch (the step index is left alone: no launch here advances it)
+        if (fp32_onchip_supported(c.geom) && fp32_fast_plane_supported(c.geom)) {
+            for (int kind = 0; kind < 2; ++kind) {
+                for (int r = 0; r < 4; ++r) {
+                    if (r == 1) CKC(cudaEventRecord(ctx->ev0, ctx->stream));
+                    if (kind == 0)
+                        fp32_plane_fast(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, ctx->d_step,
+                                        ctx->plane_occupancy, nullptr, ctx->stream);
+                    else
+                        fp32_onchip_step(c.state, c.geom, ctx->d_gparams, c.d_tgroup, c.d_tlocal, twf, c.kin_tab[1],
+                                         ctx->d_step, nullptr, ctx->stream);
+                }
+                CKC(cudaEventRecord(ctx->ev1, ctx->stream));
+                CKC(cudaEventSynchronize(ctx->ev1));
+                float ms = 0.f;
+                CKC(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+                (kind == 0 ? c.plane_ms : c.onchip_ms) = ms / 3.0;
+            }
+            c.onchip = c.onchip_ms < c.pencil_ms[c.pencil_kind] + c.plane_ms;
         }
     }
     return BEC_OK;
@@ -618,7 +662,17 @@ bec_status ensure_plan(bec_ctx *ctx)
     const int named = (int)(std::find(kPerPassNames, kPerPassNames + kPerPassCandidates, fs) - kPerPassNames);
     if (named < kPerPassCandidates) {
         cand = named;                                  // "-tma": every class on the TMA pencil kernel
-        for (auto &c : ctx->classes) c.pencil_kind = named < 2 ? kPencilRegister : kPencilTma;
+        for (auto &c : ctx->classes) {
+            c.pencil_kind = named < 2 ? kPencilRegister : kPencilTma;
+            c.onchip = false;
+        }
+        how = "forced";
+    } else if (fs == "unfused-onchip") {
+        cand = 2;                                      // register pencils, every 8x8x64 class on-chip
+        for (auto &c : ctx->classes) {
+            c.pencil_kind = kPencilRegister;
+            c.onchip = fp32_onchip_supported(c.geom);
+        }
         how = "forced";
     } else if (!fs.empty()) {
         const int k = std::atoi(fs.c_str());
@@ -627,9 +681,11 @@ bec_status ensure_plan(bec_ctx *ctx)
         cand = kPerPassCandidates + k;
         how = "forced";
     } else if (step_plan_cached(geoms, &cand)) {
-        // the candidate, and above bit 8 two bits per class: its pencil kernel
-        for (size_t ci = 0; ci < ctx->classes.size() && ci < kPickClasses; ++ci)
-            ctx->classes[ci].pencil_kind = (cand >> (8 + 2 * ci)) & 3;
+        // the candidate, and above bit 8 two bits per class: its pencil kernel, its on-chip step
+        for (size_t ci = 0; ci < ctx->classes.size() && ci < kPickClasses; ++ci) {
+            ctx->classes[ci].pencil_kind = (cand >> (8 + 2 * ci)) & 1;
+            ctx->classes[ci].onchip = (cand >> (9 + 2 * ci)) & 1;
+        }
         cand &= 0xFF;
         how = "cached";
     } else {
@@ -683,7 +739,8 @@ bec_status ensure_plan(bec_ctx *ctx)
                 how = "autotuned";
                 int picks = 0;
                 for (size_t ci = 0; ci < ctx->classes.size() && ci < kPickClasses; ++ci)
-                    picks |= ctx->classes[ci].pencil_kind << (8 + 2 * ci);
+                    picks |= (ctx->classes[ci].pencil_kind << (8 + 2 * ci)) |
+                             ((ctx->classes[ci].onchip ? 1 : 0) << (9 + 2 * ci));
                 step_plan_remember(geoms, cand | picks);
             } else {
                 cudaGetLastError();
@@ -708,10 +765,12 @@ bec_status ensure_plan(bec_ctx *ctx)
     for (auto &c : ctx->classes) {
         if (c.geom.n_traj == 0) continue;
         const int kind = ctx->pencil_tuned ? c.pencil_kind : kPencilRegister;
+        const bool oc = ctx->pencil_tuned && c.onchip && fp32_onchip_supported(c.geom);
         std::snprintf(buf, sizeof buf,
-                      "%s{\"grid\": [%d, %d, %d], \"kernel\": \"%s\", \"register_ms\": %.4f, \"tma_ms\": %.4f}",
+                      "%s{\"grid\": [%d, %d, %d], \"kernel\": \"%s\", \"register_ms\": %.4f, \"tma_ms\": %.4f, "
+                      "\"onchip\": %s, \"plane_ms\": %.4f, \"onchip_ms\": %.4f}",
                       firstc ? "" : ", ", c.geom.nx, c.geom.ny, c.geom.nz, kPencilNames[kind], c.pencil_ms[0],
-                      c.pencil_ms[1]);
+                      c.pencil_ms[1], oc ? "true" : "false", c.plane_ms, c.onchip_ms);
         j += buf;
         firstc = false;
     }

@@ -202,6 +202,12 @@ void fp32_pencil_fast(float4 *state, const ClassGeom &c, const GroupParamsF *gp,
 // = e^{+i kz_i^2/2 dt frac} for i < nz, then e^{+i (kx^2 + ky^2)/2 dt frac} per pencil (y * nx + x)
 void fp32_kin_tables(float2 *tab, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, float frac,
                      cudaStream_t s);
+// onchip_step.cu: a steady step (full kick, no pulse, no observation) of an 8x8x64 class with each trajectory's
+// state in shared memory, one launch instead of its pencil and plane launches; kin_full: the class's full-kick
+// kinetic table; inc_done as fp32_plane_fast
+bool fp32_onchip_supported(const ClassGeom &c);
+void fp32_onchip_step(float4 *state, const ClassGeom &c, const GroupParamsF *gp, const int *tgroup, const int *tlocal,
+                      const float2 *tw_full, const float2 *kin_full, uint32_t *d_step, int *inc_done, cudaStream_t s);
 // pencil_tma.cu: the non-observing pencil pass as a persistent kernel with TMA tile loads and stores
 // (bit-identical to fp32_pencil_fast); d_err: set to 1 when a wait gave up; d_never: a zero int
 bool fp32_pencil_tma_supported(const ClassGeom &c);

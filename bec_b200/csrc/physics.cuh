@@ -77,12 +77,20 @@ __device__ __forceinline__ float2 cis_taylor(float t)
 
 __device__ __forceinline__ float exp_taylor(float x) { return fmaf(x, fmaf(x, fmaf(x, 1.f / 6.f, 0.5f), 1.f), 1.f); }
 
+// |v|^2 and complex products with every fused multiply-add written out, so that every kernel that inlines the
+// cell step rounds it the same way (the contraction of a*b + c*d left to the compiler can differ between them)
+__device__ __forceinline__ float nrm2(float2 v) { return fmaf(v.x, v.x, v.y * v.y); }
+__device__ __forceinline__ float2 cmulx(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
+}
+
 // The substep's factors da, db from the midpoint estimate (xa, xb).
 __device__ __forceinline__ void nonlinear_factors(float2 xa, float2 xb, float hV, float hVd, const CellConsts &K,
                                                   float2 &da, float2 &db)
 {
-    const float na = xa.x * xa.x + xa.y * xa.y;
-    const float nb = xb.x * xb.x + xb.y * xb.y;
+    const float na = nrm2(xa);
+    const float nb = nrm2(xb);
     const float ra = fmaf(K.hl111 * na, na, K.hl12 * nb);
     const float rb = fmaf(K.hl22, nb, K.hl12 * na);
     const float ta = fmaf(K.hg11, na, fmaf(K.hg12, nb, hV));
@@ -108,22 +116,22 @@ __device__ __forceinline__ void nonlinear_factors(float2 xa, float2 xb, float hV
 __device__ __forceinline__ float4 nonlinear_cell(float4 v, float V, const CellConsts &K)
 {
     const float2 a0 = make_float2(v.x, v.y), b0 = make_float2(v.z, v.w);
-    const float hV = V * K.hdt, hVd = hV - K.hdet;
+    const float hV = __fmul_rn(V, K.hdt), hVd = __fsub_rn(hV, K.hdet);   // never contracted
     float2 da, db;
     if (K.itmax == 1) {
         // one midpoint iteration (every workload here): the factors of the start values, applied twice
         nonlinear_factors(a0, b0, hV, hVd, K, da, db);
-        const float2 ao = cmul(cmul(a0, da), da), bo = cmul(cmul(b0, db), db);
+        const float2 ao = cmulx(cmulx(a0, da), da), bo = cmulx(cmulx(b0, db), db);
         return make_float4(ao.x, ao.y, bo.x, bo.y);
     }
     float2 xa = a0, xb = b0;
     da = db = make_float2(0.f, 0.f);
     for (int it = 0; it < K.itmax; ++it) {
         nonlinear_factors(xa, xb, hV, hVd, K, da, db);
-        xa = cmul(a0, da);
-        xb = cmul(b0, db);
+        xa = cmulx(a0, da);
+        xb = cmulx(b0, db);
     }
-    const float2 ao = cmul(xa, da), bo = cmul(xb, db);
+    const float2 ao = cmulx(xa, da), bo = cmulx(xb, db);
     return make_float4(ao.x, ao.y, bo.x, bo.y);
 }
 

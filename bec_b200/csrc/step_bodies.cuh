@@ -57,7 +57,9 @@ struct VBlock {
 
 // ---------------------------------------------------------------- plane pass, N = 8, 16
 // 4 warps (128 threads); tile: 4 warps x (32 / N) planes x N^2 float4
-template <int N>
+// SMEM: `state` is a trajectory held in shared memory and `tile` is the same memory (the transposes run in
+// place): plain loads instead of L2-only ones, and the warp's loads all done before its first store.
+template <int N, bool SMEM = false>
 __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict__ state, int nz, int cells,
                                            const GroupParamsF *__restrict__ gp, const int *__restrict__ tgroup,
                                            const int *__restrict__ tlocal, uint32_t step, float4 *tile)
@@ -75,7 +77,8 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
 
     float4 v[N];
 #pragma unroll
-    for (int y = 0; y < N; ++y) v[y] = __ldcg(g + y * N + c);
+    for (int y = 0; y < N; ++y) v[y] = SMEM ? g[y * N + c] : __ldcg(g + y * N + c);
+    if (SMEM) __syncwarp();
 
     // Four transforms share one loop body (the kernel is otherwise bound by
     // instruction fetch): pass 0 forward along y, pass 1 forward along x,
@@ -96,9 +99,10 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
             // from its own shared row (a rolled loop keeps the kernel small)
 #pragma unroll
             for (int x = 0; x < N; ++x) s[c * N + (x ^ (c & 7))] = v[x];
-            const float Y = -P.ymax + P.dy * (float)c;
-            const float Z = -P.zmax + P.dz * (float)z;
-            const float base = Y * Y + Z * Z * P.inv_lambda2;
+            // coordinates and trap potential with every fused multiply-add written out (same bits in every kernel)
+            const float Y = fmaf(P.dy, (float)c, -P.ymax);
+            const float Z = fmaf(P.dz, (float)z, -P.zmax);
+            const float base = fmaf(Y, Y, (Z * Z) * P.inv_lambda2);
             const uint32_t tl = (uint32_t)tlocal[traj];
             const CellConsts K = cell_consts(P);
             const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
@@ -108,9 +112,9 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
                 float4 v0[4], o[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const float X = -P.xmax + P.dx * (float)(x + q);
+                    const float X = fmaf(P.dx, (float)(x + q), -P.xmax);
                     v0[q] = s[c * N + ((x + q) ^ (c & 7))];
-                    o[q] = nonlinear_cell(v0[q], 0.5f * (X * X + base), K);
+                    o[q] = nonlinear_cell(v0[q], 0.5f * fmaf(X, X, base), K);
                 }
                 if (P.noise) loss_noise_cell4(o, v0, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
 #pragma unroll
@@ -127,6 +131,7 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
             for (int y = 0; y < N; ++y) v[y] = s[y * N + (c ^ (y & 7))];
         }
     }
+    if (SMEM) __syncwarp();
 #pragma unroll
     for (int y = 0; y < N; ++y) g[y * N + c] = v[y];
 }
@@ -171,9 +176,9 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
         const int r = lane;
 #pragma unroll
         for (int s = 0; s < 16; ++s) tile[tix(r, kblk(s, h))] = v[s];
-        const float Y = -P.ymax + P.dy * (float)r;
-        const float Z = -P.zmax + P.dz * (float)z;
-        const float base = Y * Y + Z * Z * P.inv_lambda2;
+        const float Y = fmaf(P.dy, (float)r, -P.ymax);
+        const float Z = fmaf(P.dz, (float)z, -P.zmax);
+        const float base = fmaf(Y, Y, (Z * Z) * P.inv_lambda2);
         const uint32_t tl = (uint32_t)tlocal[traj];
         const CellConsts K = cell_consts(P);
         const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
@@ -182,11 +187,11 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
 #pragma unroll 1
         for (int s = 0; s < 16; s += 2) {
             const int x = kblk(s, h);
-            const float X0 = -P.xmax + P.dx * (float)x, X1 = -P.xmax + P.dx * (float)(x + 1);
+            const float X0 = fmaf(P.dx, (float)x, -P.xmax), X1 = fmaf(P.dx, (float)(x + 1), -P.xmax);
             float4 *s0 = tile + tix(r, x), *s1 = tile + tix(r, x + 1);
             const float4 v0 = *s0, v1 = *s1;
-            float4 o0 = nonlinear_cell(v0, 0.5f * (X0 * X0 + base), K);
-            float4 o1 = nonlinear_cell(v1, 0.5f * (X1 * X1 + base), K);
+            float4 o0 = nonlinear_cell(v0, 0.5f * fmaf(X0, X0, base), K);
+            float4 o1 = nonlinear_cell(v1, 0.5f * fmaf(X1, X1, base), K);
             if (P.noise)
                 loss_noise_cell2(o0, v0, o1, v1, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
             *s0 = o0;
@@ -238,6 +243,12 @@ struct PencilArgs {
 //          DFT over j -> k2 (k = k1 + 16 k2), kinetic phase (and pulse), forward G-point DFT, twiddle;
 //          mid_store writes it back after the caller's barrier
 //   fwd3:  thread (p, j) gathers its k1 < 16 and finishes with the forward 16-point DFT over k1 -> m
+// The buffer is a float4 pointer or an accessor (a functor mapping the buffer index to a float4 slot, e.g.
+// into a tile of a state held in shared memory).
+__device__ __forceinline__ float4 &zat(float4 *b, int i) { return b[i]; }
+template <class F>
+__device__ __forceinline__ float4 &zat(const F &f, int i) { return f(i); }
+
 template <int NZ, int PEN>
 struct ZTile {
     static constexpr int R = 16, G = NZ / 16;
@@ -245,7 +256,8 @@ struct ZTile {
 
     __device__ static __forceinline__ int bix(int p, int jj, int k1) { return (p * G + jj) * R + (k1 ^ (p & 7)); }
 
-    __device__ static __forceinline__ void inv1(float4 (&x)[R], float4 *buf, const float2 *tw, int p, int j)
+    template <class Buf>
+    __device__ static __forceinline__ void inv1(float4 (&x)[R], Buf buf, const float2 *tw, int p, int j)
     {
         dft<R, true>(x);                                            // over m -> k1 (inverse)
 #pragma unroll
@@ -254,17 +266,18 @@ struct ZTile {
             x[k1] = fftreg::cmulw(x[k1], make_float2(w.x, -w.y));   // W^{-j k1}
         }
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) buf[bix(p, j, k1)] = x[k1];
+        for (int k1 = 0; k1 < R; ++k1) zat(buf, bix(p, j, k1)) = x[k1];
     }
 
     // pxy: the pencil's (kx, ky) factor times the scale; kzp: the kz factors
-    __device__ static __forceinline__ void mid(float4 (&y)[R], const float4 *buf, const float2 *tw, const float2 *kzp,
+    template <class Buf>
+    __device__ static __forceinline__ void mid(float4 (&y)[R], Buf buf, const float2 *tw, const float2 *kzp,
                                                float2 pxy, const PencilArgs &pa, int q, int p2)
     {
 #pragma unroll
         for (int r = 0; r < R / G; ++r)
 #pragma unroll
-            for (int jj = 0; jj < G; ++jj) y[r * G + jj] = buf[bix(p2, jj, q + G * r)];
+            for (int jj = 0; jj < G; ++jj) y[r * G + jj] = zat(buf, bix(p2, jj, q + G * r));
 #pragma unroll
         for (int r = 0; r < R / G; ++r) dft<G, true>(y + r * G);   // over j -> k2: k = k1 + 16 k2
 
@@ -294,18 +307,20 @@ struct ZTile {
             for (int jj = 1; jj < G; ++jj) y[r * G + jj] = fftreg::cmulw(y[r * G + jj], tw[(q + G * r) * jj]);
     }
 
-    __device__ static __forceinline__ void mid_store(const float4 (&y)[R], float4 *buf, int q, int p2)
+    template <class Buf>
+    __device__ static __forceinline__ void mid_store(const float4 (&y)[R], Buf buf, int q, int p2)
     {
 #pragma unroll
         for (int r = 0; r < R / G; ++r)
 #pragma unroll
-            for (int jj = 0; jj < G; ++jj) buf[bix(p2, jj, q + G * r)] = y[r * G + jj];
+            for (int jj = 0; jj < G; ++jj) zat(buf, bix(p2, jj, q + G * r)) = y[r * G + jj];
     }
 
-    __device__ static __forceinline__ void fwd3(float4 (&x)[R], const float4 *buf, int p, int j)
+    template <class Buf>
+    __device__ static __forceinline__ void fwd3(float4 (&x)[R], Buf buf, int p, int j)
     {
 #pragma unroll
-        for (int k1 = 0; k1 < R; ++k1) x[k1] = buf[bix(p, j, k1)];
+        for (int k1 = 0; k1 < R; ++k1) x[k1] = zat(buf, bix(p, j, k1));
         dft<R, false>(x);
     }
 };

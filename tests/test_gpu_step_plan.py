@@ -1,5 +1,5 @@
 """The split-step schedules: per-pass launches (plane passes at 16 or 20 warps per SM; pencil passes on the
-register kernel or the persistent TMA kernel, chosen per grid class) and the
+register kernel or the persistent TMA kernel, and 8x8x64 steps as one on-chip launch, chosen per grid class) and the
 fused step kernel (one persistent launch per split step) on its autotuned work list.
 
 Every schedule computes the same bits: launches per pass and grid class, with any pencil kernel, the
@@ -31,7 +31,7 @@ GROUPS = [
 
 # forced per-pass schedules and their candidate numbers: register pencils at 16 / 20 warps per SM, then every class
 # on the TMA pencil kernel
-PER_PASS = {"unfused": 0, "unfused-20": 1, "unfused-tma": 2, "unfused-20-tma": 3}
+PER_PASS = {"unfused": 0, "unfused-20": 1, "unfused-tma": 2, "unfused-20-tma": 3, "unfused-onchip": 2}
 N_PER_PASS = 4
 N_CANDIDATES = N_PER_PASS + 5
 
@@ -70,6 +70,8 @@ def test_every_schedule_gives_the_same_bits(monkeypatch, ground_states):
             assert p["chosen"] == "forced" and p["candidate"] == PER_PASS[plan]
             want = "tma" if plan.endswith("tma") else "register"
             assert all(k["kernel"] == want for k in p["pencil_kernels"])
+            # "unfused-onchip": the 8x8x64 class's steady steps as one launch with its state in shared memory
+            assert all(k["onchip"] == (plan == "unfused-onchip" and k["grid"] == [8, 8, 64]) for k in p["pencil_kernels"])
         else:
             assert p["chosen"] == "forced" and p["candidate"] == int(plan) + N_PER_PASS
         # the fused kernel takes every class but the 2D slice
@@ -100,11 +102,18 @@ def test_autotuner_reports_timings(monkeypatch, ground_states):
         ms = p["candidate_ms_per_step"]           # the four per-pass schedules, the work lists 0..4
         assert len(ms) == N_CANDIDATES and all(v > 0 for v in ms)
         assert ms[p["candidate"]] == min(ms)
-        # per grid class, both pencil kernels were timed, and the tuned schedules use the faster
+        # per grid class, both pencil kernels were timed, and the tuned schedules use the faster; an 8x8x64
+        # class also timed its on-chip step against its pencil plus plane launches
         for k in p["pencil_kernels"]:
             ms = {name: k[name + "_ms"] for name in ("register", "tma")}
             assert all(v > 0 for v in ms.values())
-            assert k["kernel"] == (min(ms, key=ms.get) if p["candidate"] in (2, 3) else "register")
+            tuned = p["candidate"] in (2, 3)
+            assert k["kernel"] == (min(ms, key=ms.get) if tuned else "register")
+            if k["grid"] == [8, 8, 64]:
+                assert k["plane_ms"] > 0 and k["onchip_ms"] > 0
+                assert k["onchip"] == (tuned and k["onchip_ms"] < min(ms.values()) + k["plane_ms"])
+            else:
+                assert not k["onchip"]
 
 
 def test_fused_plan_is_one_launch_per_step(monkeypatch, ground_states):
