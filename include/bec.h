@@ -370,10 +370,11 @@ int32_t bec_step_graphs(const bec_ctx *ctx);
  * trajectory's plane items 0.5 to 4 waves of the grid after its pencil items -- and keeps the
  * fastest for this class mix and device (cached per process). BEC_STEP_PLAN in the environment
  * forces one (unfused, unfused-20, unfused-tma and unfused-20-tma with every class on the TMA
- * pencil kernel, or 0..4 for the work lists), BEC_AUTOTUNE=0 takes the per-pass launches untimed;
- * every schedule computes the same bits. The reference has one fixed
- * schedule of eight launches per ensemble and step (wigner.cu:178-199) with cuFFT plans built by
- * batchfftPlan3d (batchfft.cu:22-100). */
+ * pencil kernel, unfused-onchip with every 8x8x64 class's steady steps as one launch holding each
+ * trajectory in shared memory, or 0..4 for the work lists), BEC_AUTOTUNE=0 takes the per-pass launches
+ * untimed; every schedule computes the same bits. The reference has one fixed schedule of eight
+ * launches per ensemble and step (wigner.cu:178-199) with cuFFT plans built by batchfftPlan3d
+ * (batchfft.cu:22-100). */
 bec_status bec_step_plan(bec_ctx *ctx, char *out, int32_t len);
 
 /* Runs n_steps steady real-time steps (they advance the run like bec_evolve) with CUDA events on
