@@ -15,7 +15,7 @@
 // A tile is PEN = 2048 / nz adjacent pencils (32 KiB: 8 x 256, 16 x 128, 32 x 64) of one trajectory, a box
 // of {4 PEN floats, nz rows} of the class's state seen as a 2D tensor {4 nx ny floats, nz n_traj rows}.
 // 128 threads, two tile buffers, three CTAs per SM: three loads and up to three stores in flight per SM.
-// TMA loads here never multicast; a tile's source is this GPU's own memory.
+// Each TMA load feeds only the CTA that issues it, and a tile's source is this GPU's own memory.
 //
 // Every wait is bounded: a load that has not landed after the limit (BEC_STEP_WAIT_LIMIT_MS, 2 s by
 // default) sets the error flag, waits once more (bounded) for that load, drains its own stores and ends
