@@ -168,15 +168,33 @@ def mean_cells(groups):
     return sum(p.nvx * p.nvy * p.nvz * p.ne for p in groups) / max(1, sum(p.ne for p in groups))
 
 
+def host_cpu():
+    """The host's CPU model, its logical CPU count and how many of those this process may run on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_cpus": usable}
+
+
 class OracleSample:
     """A bounded sample of the workload on the CPU oracle (FP64 restatement of the
-    reference's split step), one trajectory per thread on all host cores; the sample has the
-    workload's grid-class mix."""
+    reference's split step), one trajectory per thread on all host cores the process may use;
+    the sample has the workload's grid-class mix."""
 
     def __init__(self, groups):
         from concurrent.futures import ThreadPoolExecutor
         from oracle import oracle as O
-        self.cores = os.cpu_count() or 1
+        self.cores = host_cpu()["usable_cpus"]
         self.sample = mix_sample(groups, max(3, 2 * self.cores))
         self.ens = []
         for p in self.sample:
@@ -191,6 +209,13 @@ class OracleSample:
         list(self.pool.map(lambda e: e.evolve(1, 1), self.ens))
         return time.perf_counter() - t0
 
+    def step_serial(self):
+        """The same step with every trajectory on the calling thread, one after another; returns the wall time."""
+        t0 = time.perf_counter()
+        for e in self.ens:
+            e.evolve(1, 1)
+        return time.perf_counter() - t0
+
     def describe(self, steps, seconds):
         grids = {}
         for p in self.sample:
@@ -203,14 +228,22 @@ class OracleSample:
 
 
 def cpu_baseline(groups, seconds):
-    """Oracle throughput on the sample for about `seconds`: (traj-steps/s, cores, sample)."""
+    """Oracle throughput on the sample for about `seconds` on all usable cores, then for about half as
+    long on one thread: (traj-steps/s, cores, sample, single-thread record)."""
     s = OracleSample(groups)
     s.step()
     reps = max(1, int(seconds / max(s.step(), 1e-3)))
     el = sum(s.step() for _ in range(reps))
     v = len(s.sample) * reps / el
+    first = s.step_serial()
+    reps1 = max(1, int(0.5 * seconds / max(first, 1e-3)))
+    el1 = sum(s.step_serial() for _ in range(reps1))
+    v1 = len(s.sample) * reps1 / el1
     s.close()
-    return v, s.cores, s.describe(reps, el)
+    single = {"value": v1, "unit": "traj-steps/s", "threads": 1,
+              "sample": f"the same {len(s.sample)} trajectories one after another on one thread, {reps1} steps, "
+                        f"{el1:.1f} s", "speedup_all_cores": v / v1, **host_cpu()}
+    return v, s.cores, s.describe(reps, el), single
 
 
 def run_reference(args, ws, rank):
@@ -235,7 +268,8 @@ def run_reference(args, ws, rank):
                    "grids": args.grids or "8x8x64/16x16x128/32x32x256 uniform",
                    "step": "one split step of every trajectory of a bounded sample of the workload",
                    "implementation": "CPU FP64 restatement of the reference's split step (oracle port)"},
-        "cpu_baseline": {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": sample,
+                         **host_cpu()},
         "e2e": {"value": v, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -476,9 +510,10 @@ def main():
                                 "ratio_full_batch": value / pv}
         plain.close()
         bs.close()
-        v, cores, s = cpu_baseline(groups, args.cpu_seconds)
+        v, cores, s, single = cpu_baseline(groups, args.cpu_seconds)
         cpu = {"value": v, "unit": "traj-steps/s", "cores": cores, "kind": "port", "sample": s,
-               "cell_steps_per_s": v * mean_cells(mix_sample(groups, max(3, 2 * cores)))}
+               "cell_steps_per_s": v * mean_cells(mix_sample(groups, max(3, 2 * cores))),
+               "single_thread": single}
     if rank == 0 and ws == 1 and not args.no_extras and not args.no_gs:
         extras["gs_warmstart"] = gs_warmstart_leg(args.gs_train, args.gs_eval, GS_TOL, GS_REF_TOL)
 
@@ -495,6 +530,24 @@ def main():
                           "achieved": ach, "peak": pk, "unit": "thread-instr/s", "frac": ach / pk,
                           "note": "instruction issue, the bound of this kernel: one warp-instruction per scheduler "
                                   "per clock at the sampled SM clock; instructions per cell from ncu"}
+    # the transforms' FLOPs (5 n log2 n per complex transform of n points; two components, one inverse and
+    # one forward 3D transform per step) against the FP32 FMA pipes: the compute bound beside the HBM bound
+    flop_roof = None
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if mhz:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        flops = float(np.sum(20.0 * cells * np.log2(cells)))
+        step_s = ms / args.steps * 1e-3
+        pk = sms * 128 * 2 * mhz * 1e6
+        t_flop, t_hbm = flops / pk, 32.0 * total_cells / (peak * 1e9)
+        flop_roof = {"achieved": flops / step_s / 1e12, "peak": pk / 1e12, "unit": "TFLOP/s",
+                     "frac": flops / step_s / pk, "flop_per_byte": flops / (32.0 * total_cells),
+                     "flop_time_ms": t_flop * 1e3, "hbm_time_ms": t_hbm * 1e3,
+                     "ceiling_ms": max(t_flop, t_hbm) * 1e3, "ms_per_step": ms / args.steps,
+                     "note": "whole step, this GPU's trajectories: transform FLOPs only (the cell step, Philox and "
+                             "Box-Muller add more); peak = the FP32 FMA pipes' nominal 2 flop per lane per clock at "
+                             "the sampled SM clock (the measured peaks hold no FP32 figure); ceiling = the slower of "
+                             "the FLOP and the HBM time"}
     if rank == 0:
         line = {
             "metric": "wigner_traj_steps_per_s", "value": value, "unit": "traj-steps/s",
@@ -509,6 +562,7 @@ def main():
                        "l2": f"state {16 * total_cells / 1e9:.2f} GB per GPU, larger than L2",
                        "parallelism": f"dp{ws} (trajectory sharding)", "path": "fp32-batched"},
             "roofline": roofline, "issue_roofline": issue_roof, "step_roofline": step_roof,
+            "flop_roofline": flop_roof,
             "step_plan": plan, "per_pass_kernels": per_pass, "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, **extras,

@@ -30,6 +30,7 @@ def test_reference_arm_line():
     assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    assert cb["nproc"] >= cb["usable_cpus"] == cb["cores"] >= 1 and "cpu_model" in cb
     assert d["e2e"] == {"value": d["value"], "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
@@ -54,6 +55,20 @@ def test_baseline_samples_keep_the_batch_mix():
     assert bench.mix_sample(groups[:5], 32) == groups[:5]
 
 
+def test_cpu_baseline_times_all_cores_and_one_thread():
+    """The CPU baseline times the oracle on every usable core and, on the same sample, on one thread, and
+    names the host's CPU."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from bec_b200.configs import uneven_batch
+    groups = uneven_batch(n_traj=6, seed=2, grids=[(8, 8, 64)])
+    v, cores, sample, single = bench.cpu_baseline(groups, 0.2)
+    assert v > 0 and cores == bench.host_cpu()["usable_cpus"] and "8x8x64" in sample
+    assert single["threads"] == 1 and single["value"] > 0 and single["unit"] == "traj-steps/s"
+    assert single["speedup_all_cores"] == v / single["value"]
+    assert single["nproc"] >= single["usable_cpus"] >= 1 and "one thread" in single["sample"]
+
+
 def test_rank_to_physical_gpu(monkeypatch):
     sys.path.insert(0, ROOT)
     import bench
@@ -76,3 +91,6 @@ def test_gpu_arm_line():
     assert d["gpu_launches"] > 0
     if d["clocks"] is not None:                 # None only where nvidia-smi gave no samples
         assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
+        fr = d["flop_roofline"]
+        assert fr["unit"] == "TFLOP/s" and 0 < fr["frac"] == pytest.approx(fr["achieved"] / fr["peak"])
+        assert fr["ceiling_ms"] == max(fr["flop_time_ms"], fr["hbm_time_ms"]) <= fr["ms_per_step"]
