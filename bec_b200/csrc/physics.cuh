@@ -154,12 +154,13 @@ __device__ __forceinline__ float4 loss_noise_apply(float4 out, float4 v0, const 
 
 // Adds the loss-noise increments of two cells of the same trajectory and step, evaluated at v0 and v1, to
 // out0 and out1: per cell the six normals of one Philox4x32-10 draw (loss_fields) as three complex Wiener
-// increments already scaled by their amplitudes. The two draws' rounds interleave.
+// increments already scaled by their amplitudes. The two draws' rounds interleave; keys: the round keys of
+// the ensemble seed (philox_keys).
 __device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4 &out1, float4 v1, const CellConsts &K,
-                                                 uint32_t k0, uint32_t k1, uint32_t traj, uint32_t step,
+                                                 const PhiloxKeys &keys, uint32_t traj, uint32_t step,
                                                  uint32_t cell0, uint32_t cell1)
 {
-    const u32x4x2 w = philox4x32_10_x2(cell0, step, traj, RNG_TAG_LOSS, cell1, step, traj, RNG_TAG_LOSS, k0, k1);
+    const u32x4x2 w = philox4x32_10_x2(cell0, step, traj, RNG_TAG_LOSS, cell1, step, traj, RNG_TAG_LOSS, keys);
     out0 = loss_noise_apply(out0, v0, K, w.a);
     out1 = loss_noise_apply(out1, v1, K, w.b);
 }
@@ -167,10 +168,10 @@ __device__ __forceinline__ void loss_noise_cell2(float4 &out0, float4 v0, float4
 
 // The loss-noise increments of four consecutive cells cell0 .. cell0 + 3 of the same trajectory and step:
 // one interleaved group of four Philox4x32-10 draws.
-__device__ __forceinline__ void loss_noise_cell4(float4 out[4], const float4 v0[4], const CellConsts &K, uint32_t k0,
-                                                 uint32_t k1, uint32_t traj, uint32_t step, uint32_t cell0)
+__device__ __forceinline__ void loss_noise_cell4(float4 out[4], const float4 v0[4], const CellConsts &K,
+                                                 const PhiloxKeys &keys, uint32_t traj, uint32_t step, uint32_t cell0)
 {
-    const u32x4x4 w = philox4x32_10_x4(cell0, step, traj, RNG_TAG_LOSS, k0, k1);
+    const u32x4x4 w = philox4x32_10_x4(cell0, step, traj, RNG_TAG_LOSS, keys);
     out[0] = loss_noise_apply(out[0], v0[0], K, w.a);
     out[1] = loss_noise_apply(out[1], v0[1], K, w.b);
     out[2] = loss_noise_apply(out[2], v0[2], K, w.c);

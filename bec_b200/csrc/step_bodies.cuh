@@ -106,6 +106,7 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
             const uint32_t tl = (uint32_t)tlocal[traj];
             const CellConsts K = cell_consts(P);
             const uint32_t cell0 = (uint32_t)(z * PLANE + c * N);
+            const PhiloxKeys keys = philox_keys(P.seed_lo, P.seed_hi);
             // cells in fours: the four Philox draws interleave (loss_noise_cell4)
 #pragma unroll 1
             for (int x = 0; x < N; x += 4) {
@@ -116,7 +117,7 @@ __device__ __forceinline__ void plane_body(const VBlock &vb, float4 *__restrict_
                     v0[q] = s[c * N + ((x + q) ^ (c & 7))];
                     o[q] = nonlinear_cell(v0[q], 0.5f * fmaf(X, X, base), K);
                 }
-                if (P.noise) loss_noise_cell4(o, v0, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x);
+                if (P.noise) loss_noise_cell4(o, v0, K, keys, tl, step, cell0 + x);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) s[c * N + ((x + q) ^ (c & 7))] = o[q];
             }
@@ -182,6 +183,7 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
         const uint32_t tl = (uint32_t)tlocal[traj];
         const CellConsts K = cell_consts(P);
         const uint32_t cell0 = (uint32_t)(z * 1024 + r * 32);
+        const PhiloxKeys keys = philox_keys(P.seed_lo, P.seed_hi);
         // cells in pairs (x, x + 1; kblk keeps pairs of even s adjacent): the two Philox draws interleave.
         // (Fours measured slower here: the larger loop body misses in the instruction cache.)
 #pragma unroll 1
@@ -193,7 +195,7 @@ __device__ __forceinline__ void plane32_body(const VBlock &vb, float4 *__restric
             float4 o0 = nonlinear_cell(v0, 0.5f * fmaf(X0, X0, base), K);
             float4 o1 = nonlinear_cell(v1, 0.5f * fmaf(X1, X1, base), K);
             if (P.noise)
-                loss_noise_cell2(o0, v0, o1, v1, K, P.seed_lo, P.seed_hi, tl, step, cell0 + x, cell0 + x + 1);
+                loss_noise_cell2(o0, v0, o1, v1, K, keys, tl, step, cell0 + x, cell0 + x + 1);
             *s0 = o0;
             *s1 = o1;
         }
