@@ -29,12 +29,12 @@ sys.path.insert(0, ROOT)
 # ncu: DRAM bytes (read + write) per cell of one launch of a pass kernel, from a capture of 64 x 32x32x256
 # trajectories (268 MB of state, larger than L2; dram__bytes_read.sum + dram__bytes_write.sum over the launch's
 # cells); traffic scales with the cells a launch processes (algorithmic: 32 B per cell).
-NCU_TRAFFIC_PER_CELL = {"plane_32x32x256": 28.43, "pencil_32x32x256": 28.49}
+NCU_TRAFFIC_PER_CELL = {"plane_32x32x256": 28.44, "pencil_32x32x256": 28.47}
 
 # ncu: thread-instructions per cell of one launch (smsp__inst_executed.sum x 32 / cells), from the same
 # capture. With the launch time they give the kernel's instruction issue rate, whose ceiling is one
 # warp-instruction per scheduler per clock: SMs x 4 x 32 thread-instructions per clock.
-NCU_INSTR_PER_CELL = {"plane_32x32x256": 354.0, "pencil_32x32x256": 131.8}
+NCU_INSTR_PER_CELL = {"plane_32x32x256": 354.9, "pencil_32x32x256": 131.8}
 
 N_TRAJ = 1024
 # stopping rules of the ground-state leg: |d mu|/mu between checks below 1e-7 stops every held-out set
