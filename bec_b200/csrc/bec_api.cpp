@@ -2066,6 +2066,9 @@ bec_status bec_evolve(bec_ctx *ctx, int32_t n_steps)
     if (n_steps < 0) return fail(ctx, BEC_ERR_INVALID_ARG, "negative step count");
     bec_status st = check_ready(ctx);
     if (st) return st;
+    // the schedule autotuner times its candidates with the same events; it normally runs in the equilibration
+    // step of bec_start_evolution, and never inside this call's timed region
+    if ((st = ensure_plan(ctx))) return st;
     const long long l0 = g_launches;
     CKC(cudaEventRecord(ctx->ev0, ctx->stream));
     if ((st = do_evolve(ctx, n_steps))) return st;

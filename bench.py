@@ -395,7 +395,7 @@ def main():
     total_cells = float(cells.sum())
 
     # warm-up, then K device-timed steps
-    eng.evolve(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+    eng.evolve(args.warmup)     # the first steps also run the schedule autotuner
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
