@@ -10,6 +10,7 @@ import pytest
 from bec_b200 import warmstart as W
 from bec_b200._abi import BEC_GS_FIXED_STEPS, BEC_GS_MU_RESIDUAL
 from bec_b200.configs import rb87_params
+from parity_util import record
 
 
 def _family(n, seed, m=2000):
@@ -119,6 +120,8 @@ def test_installed_basis_projection_and_warm_start():
 def test_warm_start_pipeline_beats_cold_start():
     out = W.run(n_train=512, n_eval=32, n_pod=128, seed=5, train_steps=1500, tol=1e-6, grid=(16, 16, 128),
                 log=lambda *a: None)
+    record("warm_start_pipeline_16x16x128", speedup_steps=out["speedup_steps"],
+           mu_rel_diff_max=out["mu_rel_diff_max"])
     assert out["cold_converged"] == 1.0 and out["warm_converged"] == 1.0
     assert out["speedup_steps"] > 3.0
     assert out["mu_rel_diff_max"] < 2e-5
