@@ -1149,9 +1149,9 @@ bec_status bec_create(const bec_params *groups, int32_t n_groups, int32_t path, 
     bec_status st = BEC_OK;
     auto bail = [&](bec_status s) { bec_destroy(ctx); return s; };
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BEC_ERR_CUDA);
-    cudaEventCreate(&ctx->ev0);
-    cudaEventCreate(&ctx->ev1);
-    cudaEventCreateWithFlags(&ctx->ev_h2d, cudaEventDisableTiming);
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_h2d, cudaEventDisableTiming) != cudaSuccess)
+        return bail(BEC_ERR_CUDA);
 
     // trajectory numbering: classes in first-appearance order, groups in order within a class
     if (path == BEC_PATH_FP32_BATCHED) {
@@ -2483,6 +2483,7 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
     const bool plain = ctx->path == BEC_PATH_FP64_PLAIN;
     const int nc = plain ? (int)ctx->groups.size() : (int)ctx->classes.size();
     std::vector<cudaEvent_t> ev;
+    struct Destroy { std::vector<cudaEvent_t> &v; ~Destroy() { for (cudaEvent_t e : v) cudaEventDestroy(e); } } destroy{ev};
     auto new_event = [&]() { cudaEvent_t e; cudaEventCreate(&e); ev.push_back(e); return e; };
     // [step][class][pass] -> (start, stop)
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks((size_t)n_steps * nc * 2, {nullptr, nullptr});
@@ -2542,7 +2543,6 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
         }
     }
     *n_classes = nc;
-    for (cudaEvent_t e : ev) cudaEventDestroy(e);
     return BEC_OK;
 }
 
