@@ -15,6 +15,10 @@ RB87_MASS = 1.443160648e-25
 A11, A12, A22 = 100.40, 97.66, 95.00
 FX, FY, FZ = 97.6, 97.6, 11.96
 GAMMA111, GAMMA12, GAMMA22 = 5.4e-42, 1.51e-20, 8.1e-20
+# The loss rates written, commented out, in the reference's parameter set (wigner.cpp:74-76: 5.4e-30 cm^6/s,
+# 0.78e-13 cm^3/s, 1.194e-13 cm^3/s), in SI units. The stored GPU curve data/gpu_sp_30k.yaml (30k atoms, no
+# noise) is reproduced with these over its whole 0.6 s, and not with the rates above.
+SOURCE_GAMMA111, SOURCE_GAMMA12, SOURCE_GAMMA22 = 5.4e-42, 0.78e-19, 1.194e-19
 
 
 def rb87_params(N=30000.0, grid=(16, 16, 128), ne=1, noise=False, losses=True,
