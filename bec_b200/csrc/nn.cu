@@ -8,8 +8,13 @@
 // Layers are Y = act(X W^T + b) (W is [out x in], row-major, as a linear layer),
 // tanh on hidden layers, identity on the last. GEMMs run on the 5th-generation
 // tensor cores (tcgen05.mma, BF16 operands from shared memory, FP32 accumulator in
-// tensor memory); master weights, Adam moments, activations' pre-images and
-// gradients are FP32.
+// tensor memory) with split operands: every FP32 operand x is held as two BF16
+// values, hi = bf16(x) and lo = bf16(x - hi), and a product is accumulated as
+// hi*hi + hi*lo + lo*hi (three MMAs), about 16 significant bits per operand instead
+// of 8. Single BF16 products limited the trained network (its loss stalled at the
+// BF16 rounding level and its warm starts needed 1.6x the steps of the same
+// network trained in FP32). Master weights, Adam moments, activations' pre-images
+// and gradients are FP32.
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
@@ -25,19 +30,20 @@
 namespace {
 
 // ---------------------------------------------------------------- GEMM on the 5th-generation tensor cores
-// C[M x N] = A[M x K] * B[N x K]^T (+ bias[N]); A, B BF16 row-major (K contiguous), C FP32; M, N, K multiples of 64.
-// One CTA of 128 threads per 128 x 64 tile of C. The FP32 accumulator lives in tensor memory (64 columns, lane i =
-// row i of the tile). K runs in groups of up to four 64-wide stages: the threads copy every stage's A and B tiles
-// to shared memory at once (cp.async, 16 bytes each) in the K-major canonical layout without swizzle (8-row x
-// 16-byte core matrices; the two 16-byte K chunks of one instruction 128 B apart, consecutive 8-row groups 1024 B
-// apart), then one thread issues four tcgen05.mma (M 128, N 64, K 16, BF16 in, FP32 accumulate) per stage and
-// tcgen05.commit arrives on an mbarrier when they are done; every wait is bounded. Rows of a last 64-row tile
-// (M = 64 mod 128) are zero in A and not stored. The epilogue reads the accumulator with tcgen05.ld (warp w owns
-// lanes 32w..32w+31), adds the bias and stores FP32 rows.
+// C[M x N] = A[M x K] * B[N x K]^T (+ bias[N]) with A = A_hi + A_lo, B = B_hi + B_lo (BF16 row-major, K contiguous);
+// C FP32; M, N, K multiples of 64. One CTA of 128 threads per 128 x 64 tile of C. The FP32 accumulator lives in
+// tensor memory (64 columns, lane i = row i of the tile). K runs in groups of up to four 64-wide stages: the threads
+// copy every stage's four tiles (A and B, hi and lo) to shared memory at once (cp.async, 16 bytes each) in the
+// K-major canonical layout without swizzle (8-row x 16-byte core matrices; the two 16-byte K chunks of one
+// instruction 128 B apart, consecutive 8-row groups 1024 B apart), then one thread issues, per 16-wide K step, the
+// three tcgen05.mma (M 128, N 64, K 16, BF16 in, FP32 accumulate) lo*hi, hi*lo, hi*hi, and tcgen05.commit arrives
+// on an mbarrier when they are done; every wait is bounded. Rows of a last 64-row tile (M = 64 mod 128) are zero in
+// A and not stored. The epilogue reads the accumulator with tcgen05.ld (warp w owns lanes 32w..32w+31), adds the
+// bias and stores FP32 rows.
 constexpr int GM = 128, GN = 64, GK = 64, GSTAGES = 4;
-constexpr int kStageBytes = (GM + GN) * GK * 2;               // A 16 KiB + B 8 KiB
-constexpr int kGemmSmem = GSTAGES * kStageBytes + 64;       // + mbarrier and TMEM slot: 96 KiB, at most two CTAs
-                                                            // (128 of the 512 TMEM columns) per SM
+constexpr int kTileA = GM * GK * 2, kTileB = GN * GK * 2;     // 16 KiB, 8 KiB
+constexpr int kStageBytes = 2 * (kTileA + kTileB);          // hi and lo of both: 48 KiB
+constexpr int kGemmSmem = GSTAGES * kStageBytes + 64;       // + mbarrier and TMEM slot: 192 KiB, one CTA per SM
 // instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
 // N >> 3 at bits 17-22, M >> 4 at bits 24-28
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(GN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
@@ -91,13 +97,23 @@ __device__ __noinline__ bool wait_flag(const int *flag, unsigned long long limit
     return true;
 }
 
-__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, const __nv_bfloat16 *__restrict__ B,
+// one tcgen05.mma of the tile: D (+)= A B^T from the shared-memory descriptors; accumulate = 0 overwrites D
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(tmem), "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, const __nv_bfloat16 *__restrict__ Alo,
+                                                 const __nv_bfloat16 *__restrict__ B, const __nv_bfloat16 *__restrict__ Blo,
                                                  float *__restrict__ C, const float *__restrict__ bias, int M, int N,
                                                  int K, int *err, const int *never, int stall,
                                                  unsigned long long limit_ns)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
-    // stage g: A tile (128 rows x 64 K) at g * kStageBytes, B tile (64 rows x 64 K) 16 KiB after it
+    // stage g at g * kStageBytes: A_hi (128 rows x 64 K), B_hi (64 rows x 64 K), A_lo, B_lo
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + GSTAGES * kStageBytes);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + GSTAGES * kStageBytes + 8);
     const int t = threadIdx.x, warp = t >> 5;
@@ -124,19 +140,24 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict
         // row c % 8; A rows past M are zero-filled (source size 0)
         for (int g = 0; g < stages; ++g) {
             const int k0 = kg + g * GK;
-            unsigned char *As = sm + g * kStageBytes, *Bs = As + GM * GK * 2;
+            unsigned char *As = sm + g * kStageBytes, *Bs = As + kTileA, *Als = Bs + kTileB, *Bls = Als + kTileA;
             for (int c = t; c < GM * 8; c += 128) {
                 const int row = (c >> 6) * 8 + (c & 7), kc = (c >> 3) & 7;
                 const bool in = m0 + row < M;
-                const __nv_bfloat16 *src = A + (size_t)(in ? m0 + row : 0) * K + k0 + kc * 8;
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(As + 16 * c)), "l"(src),
+                const size_t off = (size_t)(in ? m0 + row : 0) * K + k0 + kc * 8;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(As + 16 * c)), "l"(A + off),
+                             "r"(in ? 16 : 0)
+                             : "memory");
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(Als + 16 * c)), "l"(Alo + off),
                              "r"(in ? 16 : 0)
                              : "memory");
             }
             for (int c = t; c < GN * 8; c += 128) {
                 const int row = (c >> 6) * 8 + (c & 7), kc = (c >> 3) & 7;
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(Bs + 16 * c)),
-                             "l"(B + (size_t)(n0 + row) * K + k0 + kc * 8)
+                const size_t off = (size_t)(n0 + row) * K + k0 + kc * 8;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(Bs + 16 * c)), "l"(B + off)
+                             : "memory");
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(Bls + 16 * c)), "l"(Blo + off)
                              : "memory");
             }
         }
@@ -146,15 +167,16 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             for (int g = 0; g < stages; ++g) {
-                const uint32_t as = saddr(sm + g * kStageBytes), bs = as + GM * GK * 2;
+                const uint32_t as = saddr(sm + g * kStageBytes), bs = as + kTileA, als = bs + kTileB,
+                               bls = als + kTileA;
 #pragma unroll
                 for (int kk = 0; kk < GK / 16; ++kk) {
                     const uint64_t ad = kmajor_desc(as + 256 * kk), bd = kmajor_desc(bs + 256 * kk);
-                    const uint32_t accumulate = (kg > 0 || g > 0 || kk > 0) ? 1u : 0u;
-                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                                 ::"r"(tmem), "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate)
-                                 : "memory");
+                    const uint64_t ald = kmajor_desc(als + 256 * kk), bld = kmajor_desc(bls + 256 * kk);
+                    // the small products first; only the very first MMA of the tile starts D afresh
+                    mma_f16(tmem, ald, bd, (kg > 0 || g > 0 || kk > 0) ? 1u : 0u);
+                    mma_f16(tmem, ad, bld, 1u);
+                    mma_f16(tmem, ad, bd, 1u);
                 }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -210,13 +232,20 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
 }
 
-// y = tanh(z) (or z on the output layer) as BF16 for the next GEMM, FP32 copy kept
-__global__ void k_act(const float *z, float *y, __nv_bfloat16 *ybf, size_t n, int linear)
+// the split of an FP32 value into hi = bf16(v) and lo = bf16(v - hi)
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __float2bfloat16(v);
+    lo = __float2bfloat16(v - __bfloat162float(hi));
+}
+
+// y = tanh(z) (or z on the output layer), FP32, and its split (yhi, ylo) for the next GEMM
+__global__ void k_act(const float *z, float *y, __nv_bfloat16 *yhi, __nv_bfloat16 *ylo, size_t n, int linear)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = linear ? z[i] : tanhf(z[i]);
         y[i] = v;
-        if (ybf) ybf[i] = __float2bfloat16(v);
+        split_bf16(v, yhi[i], ylo[i]);
     }
 }
 
@@ -227,13 +256,14 @@ __global__ void k_act_back(const float *dy, const float *y, float *dz, size_t n,
         dz[i] = linear ? dy[i] : dy[i] * (1.0f - y[i] * y[i]);
 }
 
-// out[c][r] = bf16(in[r][c]) for an R x Cn FP32 matrix (also plain casts with transpose = 0)
-__global__ void k_cast_t(const float *in, __nv_bfloat16 *out, int R, int Cn, int transpose)
+// (hi, lo)[c][r] = split(in[r][c]) for an R x Cn FP32 matrix (also plain splits with transpose = 0)
+__global__ void k_cast_t(const float *in, __nv_bfloat16 *hi, __nv_bfloat16 *lo, int R, int Cn, int transpose)
 {
     const size_t n = (size_t)R * Cn;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int r = (int)(i / Cn), c = (int)(i - (size_t)r * Cn);
-        out[transpose ? (size_t)c * R + r : i] = __float2bfloat16(in[i]);
+        const size_t o = transpose ? (size_t)c * R + r : i;
+        split_bf16(in[i], hi[o], lo[o]);
     }
 }
 
@@ -297,13 +327,13 @@ struct bec_mlp {
     std::vector<size_t> woff, boff;  // offsets into the parameter vector
     size_t n_params = 0;
     float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // FP32 params, grads, Adam moments
-    __nv_bfloat16 *pbf = nullptr;    // BF16 weights [out x in]
-    __nv_bfloat16 *wt = nullptr;     // scratch for W^T
+    __nv_bfloat16 *pbf = nullptr, *plo = nullptr;   // the weights' split [out x in] (hi, lo)
+    __nv_bfloat16 *wt = nullptr, *wtlo = nullptr;   // scratch for the split of W^T
     int cap = 0;                     // batch capacity of the activation buffers
     std::vector<float *> z, y;       // per layer: pre-activation, activation (FP32) [cap x w]
-    std::vector<__nv_bfloat16 *> xbf; // per layer input in BF16 [cap x w]
+    std::vector<__nv_bfloat16 *> xbf, xlo;   // per layer the input's split [cap x w]
     float *dy = nullptr, *dz = nullptr, *loss = nullptr;
-    __nv_bfloat16 *tA = nullptr, *tB = nullptr;
+    __nv_bfloat16 *tA = nullptr, *tB = nullptr, *tAlo = nullptr, *tBlo = nullptr;   // split scratch operands
     int *idx = nullptr;
     int *d_err = nullptr;            // [0] set by a GEMM whose wait ran out, [1] a flag nothing sets
     float *xin = nullptr, *tgt = nullptr;
@@ -333,24 +363,28 @@ bec_status mlp_reserve(bec_mlp *m, int batch)
     m->z.assign(m->L + 1, nullptr);
     m->y.assign(m->L + 1, nullptr);
     m->xbf.assign(m->L + 1, nullptr);
+    m->xlo.assign(m->L + 1, nullptr);
     bec_status st;
     for (int l = 0; l <= m->L; ++l) {
         if ((st = mlp_alloc(m, (void **)&m->z[l], sizeof(float) * cap * m->w[l]))) return st;
         if ((st = mlp_alloc(m, (void **)&m->y[l], sizeof(float) * cap * m->w[l]))) return st;
         if ((st = mlp_alloc(m, (void **)&m->xbf[l], sizeof(__nv_bfloat16) * cap * m->w[l]))) return st;
+        if ((st = mlp_alloc(m, (void **)&m->xlo[l], sizeof(__nv_bfloat16) * cap * m->w[l]))) return st;
     }
     if ((st = mlp_alloc(m, (void **)&m->dy, sizeof(float) * cap * maxw))) return st;
     if ((st = mlp_alloc(m, (void **)&m->dz, sizeof(float) * cap * maxw))) return st;
     if ((st = mlp_alloc(m, (void **)&m->tA, sizeof(__nv_bfloat16) * cap * maxw))) return st;
     if ((st = mlp_alloc(m, (void **)&m->tB, sizeof(__nv_bfloat16) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->tAlo, sizeof(__nv_bfloat16) * cap * maxw))) return st;
+    if ((st = mlp_alloc(m, (void **)&m->tBlo, sizeof(__nv_bfloat16) * cap * maxw))) return st;
     if ((st = mlp_alloc(m, (void **)&m->tgt, sizeof(float) * cap * m->w[m->L]))) return st;
     m->cap = cap;
     return BEC_OK;
 }
 
-// C[M x N] = A[M x K] B[N x K]^T (+ bias) on m's stream
-void gemm_bt(bec_mlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *C, const float *bias, int M, int N,
-             int K)
+// C[M x N] = A[M x K] B[N x K]^T (+ bias) on m's stream; A and B each as their split (hi, lo)
+void gemm_bt(bec_mlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *Alo, const __nv_bfloat16 *B,
+             const __nv_bfloat16 *Blo, float *C, const float *bias, int M, int N, int K)
 {
     ensure_smem_limit((const void *)k_gemm_tc, kGemmSmem);
     // BEC_STEP_WAIT_LIMIT_MS bounds the device-side waits (2 s by default); BEC_GEMM_INJECT_STALL=1 makes the
@@ -360,7 +394,8 @@ void gemm_bt(bec_mlp *m, const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *
     const char *inj = std::getenv("BEC_GEMM_INJECT_STALL");
     const int stall = inj && std::atoi(inj) ? 1 : 0;
     dim3 grid(N / GN, (M + GM - 1) / GM);
-    k_gemm_tc<<<grid, 128, kGemmSmem, m->s>>>(A, B, C, bias, M, N, K, m->d_err, m->d_err + 1, stall, limit_ns);
+    k_gemm_tc<<<grid, 128, kGemmSmem, m->s>>>(A, Alo, B, Blo, C, bias, M, N, K, m->d_err, m->d_err + 1, stall,
+                                             limit_ns);
     g_launches++;
 }
 
@@ -385,12 +420,13 @@ bec_status check_gemm(bec_mlp *m)
 void mlp_forward_dev(bec_mlp *m, int rows)
 {
     cudaStream_t s = m->s;
-    k_cast_t<<<grid_for((size_t)rows * m->w[0]), 256, 0, s>>>(m->y[0], m->xbf[0], rows, m->w[0], 0);
+    k_cast_t<<<grid_for((size_t)rows * m->w[0]), 256, 0, s>>>(m->y[0], m->xbf[0], m->xlo[0], rows, m->w[0], 0);
     for (int l = 0; l < m->L; ++l) {
         const int in = m->w[l], out = m->w[l + 1];
-        gemm_bt(m, m->xbf[l], m->pbf + m->woff[l], m->z[l + 1], m->p + m->boff[l], rows, out, in);
+        gemm_bt(m, m->xbf[l], m->xlo[l], m->pbf + m->woff[l], m->plo + m->woff[l], m->z[l + 1], m->p + m->boff[l],
+                rows, out, in);
         const int linear = (l == m->L - 1);
-        k_act<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->z[l + 1], m->y[l + 1], m->xbf[l + 1],
+        k_act<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->z[l + 1], m->y[l + 1], m->xbf[l + 1], m->xlo[l + 1],
                                                            (size_t)rows * out, linear);
         g_launches++;
     }
@@ -411,15 +447,15 @@ void mlp_backward_dev(bec_mlp *m, int rows, int valid)
         k_act_back<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dy, m->y[l + 1], m->dz, (size_t)rows * out, linear);
         k_colsum<<<(out + 127) / 128, 128, 0, s>>>(m->dz, m->g + m->boff[l], rows, out);
         // dW [out x in] = dZ^T [out x rows] * (X^T [in x rows])^T
-        k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 1);
-        k_cast_t<<<grid_for((size_t)rows * in), 256, 0, s>>>(m->y[l], m->tB, rows, in, 1);
-        gemm_bt(m, m->tA, m->tB, m->g + m->woff[l], nullptr, out, in, rows);
+        k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, m->tAlo, rows, out, 1);
+        k_cast_t<<<grid_for((size_t)rows * in), 256, 0, s>>>(m->y[l], m->tB, m->tBlo, rows, in, 1);
+        gemm_bt(m, m->tA, m->tAlo, m->tB, m->tBlo, m->g + m->woff[l], nullptr, out, in, rows);
         g_launches += 4;
         if (l > 0) {
             // dX [rows x in] = dZ [rows x out] * W [out x in] = dZ * (W^T [in x out])^T
-            k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, rows, out, 0);
-            k_cast_t<<<grid_for((size_t)out * in), 256, 0, s>>>(m->p + m->woff[l], m->wt, out, in, 1);
-            gemm_bt(m, m->tA, m->wt, m->dy, nullptr, rows, in, out);
+            k_cast_t<<<grid_for((size_t)rows * out), 256, 0, s>>>(m->dz, m->tA, m->tAlo, rows, out, 0);
+            k_cast_t<<<grid_for((size_t)out * in), 256, 0, s>>>(m->p + m->woff[l], m->wt, m->wtlo, out, in, 1);
+            gemm_bt(m, m->tA, m->tAlo, m->wt, m->wtlo, m->dy, nullptr, rows, in, out);
             g_launches += 2;
         }
     }
@@ -429,7 +465,8 @@ void mlp_sync_bf16(bec_mlp *m)
 {
     for (int l = 0; l < m->L; ++l) {
         k_cast_t<<<grid_for((size_t)m->w[l] * m->w[l + 1]), 256, 0, m->s>>>(m->p + m->woff[l], m->pbf + m->woff[l],
-                                                                             m->w[l + 1], m->w[l], 0);
+                                                                             m->plo + m->woff[l], m->w[l + 1], m->w[l],
+                                                                             0);
         g_launches++;
     }
 }
@@ -477,9 +514,11 @@ bec_status bec_mlp_create(const int32_t *widths, int32_t n_layers, uint64_t seed
     if ((st = mlp_alloc(m, (void **)&m->m, sizeof(float) * m->n_params))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->v, sizeof(float) * m->n_params))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->pbf, sizeof(__nv_bfloat16) * m->n_params))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->plo, sizeof(__nv_bfloat16) * m->n_params))) return bail(st);
     int maxw = 0;
     for (int v : m->w) maxw = std::max(maxw, v);
     if ((st = mlp_alloc(m, (void **)&m->wt, sizeof(__nv_bfloat16) * maxw * maxw))) return bail(st);
+    if ((st = mlp_alloc(m, (void **)&m->wtlo, sizeof(__nv_bfloat16) * maxw * maxw))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->loss, sizeof(float)))) return bail(st);
     if ((st = mlp_alloc(m, (void **)&m->d_err, 2 * sizeof(int)))) return bail(st);
     if (cudaMemsetAsync(m->d_err, 0, 2 * sizeof(int), m->s) != cudaSuccess) return bail(BEC_ERR_CUDA);

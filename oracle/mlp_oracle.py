@@ -1,10 +1,15 @@
 """FP64 NumPy oracle of the warm-start MLP (test infrastructure only).
 
 Layers y = act(x W^T + b), tanh on hidden layers, identity on the last, loss
-mean((y - t)^2). With bf16=True every GEMM operand is rounded to bfloat16 the
-way the GPU kernels round it (round to nearest even on the float32 value):
-the layer inputs, the weights, the backpropagated dZ, the transposed layer
-inputs and W^T; everything else stays FP64.
+mean((y - t)^2). The GEMM operands are the layer inputs, the weights, the
+backpropagated dZ, the transposed layer inputs and W^T; arith says how a GEMM
+treats them, everything else staying FP64:
+  "fp64"   plain FP64 products;
+  "bf16"   every operand rounded to bfloat16 (round to nearest even on its
+           float32 value);
+  "split"  the GPU kernels' arithmetic: every operand v (a float32 value) as
+           hi = bf16(v) and lo = bf16(v - hi), the product accumulated as
+           hi*hi + hi*lo + lo*hi (the lo*lo term dropped).
 """
 import numpy as np
 
@@ -33,20 +38,38 @@ def pack(Ws, bs):
     return np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in zip(Ws, bs)])
 
 
-def forward(params, widths, x, bf16=False):
+def split_bf16(a):
+    """hi = bf16(v), lo = bf16(v - hi) of the float32 values v of a (v - hi is exact in float32)."""
+    f = np.ascontiguousarray(a, dtype=np.float32).astype(np.float64)
+    hi = to_bf16(f)
+    return hi, to_bf16(f - hi)
+
+
+def matmul(a, b, arith="fp64"):
+    """a @ b with the operands treated as arith says."""
+    if arith == "fp64":
+        return np.asarray(a, dtype=np.float64) @ np.asarray(b, dtype=np.float64)
+    if arith == "bf16":
+        return to_bf16(a) @ to_bf16(b)
+    if arith == "split":
+        ah, al = split_bf16(a)
+        bh, bl = split_bf16(b)
+        return al @ bh + ah @ bl + ah @ bh
+    raise ValueError(arith)
+
+
+def forward(params, widths, x, arith="fp64"):
     Ws, bs = unpack(params, widths)
-    r = to_bf16 if bf16 else (lambda a: np.asarray(a, dtype=np.float64))
     ys = [np.asarray(x, dtype=np.float64)]
     for l, (W, b) in enumerate(zip(Ws, bs)):
-        z = r(ys[-1]) @ r(W).T + b
+        z = matmul(ys[-1], W.T, arith) + b
         ys.append(z if l == len(Ws) - 1 else np.tanh(z))
     return ys
 
 
-def loss_and_grads(params, widths, x, t, bf16=False):
+def loss_and_grads(params, widths, x, t, arith="fp64"):
     Ws, bs = unpack(params, widths)
-    r = to_bf16 if bf16 else (lambda a: np.asarray(a, dtype=np.float64))
-    ys = forward(params, widths, x, bf16)
+    ys = forward(params, widths, x, arith)
     B, O = ys[-1].shape
     d = ys[-1] - np.asarray(t, dtype=np.float64)
     loss = float((d * d).mean())
@@ -55,7 +78,7 @@ def loss_and_grads(params, widths, x, t, bf16=False):
     for l in range(len(Ws) - 1, -1, -1):
         dz = dy if l == len(Ws) - 1 else dy * (1.0 - ys[l + 1] ** 2)
         gb[l] = dz.sum(axis=0)
-        gW[l] = r(dz).T @ r(ys[l])
+        gW[l] = matmul(dz.T, ys[l], arith)
         if l > 0:
-            dy = r(dz) @ r(Ws[l])
+            dy = matmul(dz, Ws[l], arith)
     return loss, pack(gW, gb)

@@ -1,11 +1,12 @@
 """The warm-start MLP: the FP64 oracle against finite differences (CPU), and the
-GPU forward/backward kernels (BF16 tensor-core GEMMs, FP32 accumulation)
-against the oracle (GPU, called through the C ABI).
+GPU forward/backward kernels (tensor-core GEMMs on split BF16 operands, FP32
+accumulation) against the oracle (GPU, called through the C ABI).
 
-Tolerances: the GPU rounds GEMM operands to bfloat16 exactly as the oracle's
-bf16 mode does, so the remaining differences are FP32 accumulation order and
-tanh in FP32: relative 2e-3 on gradients and outputs against the bf16-mode
-oracle, 3e-2 against plain FP64."""
+Tolerances: the GPU splits GEMM operands into two bfloat16 values exactly as the
+oracle's split mode does, so the remaining differences are FP32 accumulation
+order and tanh in FP32: relative 1e-4 on gradients and outputs against the
+split-mode oracle, 1e-3 against plain FP64 (single bfloat16 operands, the
+oracle's bf16 mode, are ~1e-2 from FP64)."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,23 @@ def test_bf16_rounding():
     assert r[4] == 0.0
 
 
+def test_split_operands_carry_16_bits():
+    """hi + lo reconstructs a float32 value within 2^-16 of it, and split products bring the oracle's
+    gradients an order of magnitude or more closer to FP64 than single bfloat16 operands."""
+    rng = np.random.default_rng(7)
+    v = (rng.standard_normal(10000) * np.exp(rng.uniform(-8, 8, 10000))).astype(np.float32)
+    hi, lo = M.split_bf16(v)
+    assert np.all(np.abs(hi + lo - v) <= 2.0 ** -16 * np.abs(v))
+    assert np.all(M.to_bf16(hi) == hi) and np.all(M.to_bf16(lo) == lo)
+    x, t = _data(64)
+    p = _params(WIDTHS).astype(np.float64)
+    _, g64 = M.loss_and_grads(p, WIDTHS, x, t)
+    _, gs = M.loss_and_grads(p, WIDTHS, x, t, arith="split")
+    _, gb = M.loss_and_grads(p, WIDTHS, x, t, arith="bf16")
+    es, eb = (np.linalg.norm(g - g64) / np.linalg.norm(g64) for g in (gs, gb))
+    assert es < 1e-3 and es < eb / 10, (es, eb)
+
+
 def test_oracle_gradients_match_finite_differences():
     widths = [3, 8, 8, 4]
     x, t = _data(7, seed=3, widths=widths)
@@ -61,17 +79,21 @@ def test_gpu_forward_and_gradients_match_oracle():
     net.set_params(p)
     np.testing.assert_array_equal(net.get_params(), p)
     y = net.forward(x)
-    y_o = M.forward(p, WIDTHS, x, bf16=True)[-1]
-    assert np.abs(y - y_o).max() < 2e-3 * np.abs(y_o).max()
+    y_o = M.forward(p, WIDTHS, x, arith="split")[-1]
+    y64 = M.forward(p, WIDTHS, x)[-1]
     loss, g = net.gradients(x, t)
-    loss_o, g_o = M.loss_and_grads(p, WIDTHS, x, t, bf16=True)
-    assert loss == pytest.approx(loss_o, rel=2e-3)
-    assert np.linalg.norm(g - g_o) < 2e-3 * np.linalg.norm(g_o)
-    _, g64 = M.loss_and_grads(p, WIDTHS, x, t, bf16=False)
-    assert np.linalg.norm(g - g64) < 3e-2 * np.linalg.norm(g64)
+    loss_o, g_o = M.loss_and_grads(p, WIDTHS, x, t, arith="split")
+    _, g64 = M.loss_and_grads(p, WIDTHS, x, t)
     from parity_util import record
-    record("mlp_grad", rel_err_bf16=np.linalg.norm(g - g_o) / np.linalg.norm(g_o),
+    record("mlp_grad", out_err_split=np.abs(y - y_o).max() / np.abs(y_o).max(),
+           rel_err_split=np.linalg.norm(g - g_o) / np.linalg.norm(g_o),
+           out_err_fp64=np.abs(y - y64).max() / np.abs(y64).max(),
            rel_err_fp64=np.linalg.norm(g - g64) / np.linalg.norm(g64))
+    assert np.abs(y - y_o).max() < 1e-4 * np.abs(y_o).max()
+    assert loss == pytest.approx(loss_o, rel=1e-4)
+    assert np.linalg.norm(g - g_o) < 1e-4 * np.linalg.norm(g_o)
+    assert np.abs(y - y64).max() < 1e-3 * np.abs(y64).max()
+    assert np.linalg.norm(g - g64) < 1e-3 * np.linalg.norm(g64)
 
 
 @pytest.mark.gpu
