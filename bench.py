@@ -40,7 +40,7 @@ N_TRAJ = 1024
 # stopping rules of the ground-state leg: |d mu|/mu between checks below 1e-7 stops every held-out set
 # within 1e-6 of its converged mu (measured); 1e-6 is the reference-style test on the change alone
 GS_TOL, GS_REF_TOL = 1e-7, 1e-6
-GS_TRAIN_STEPS = 60000     # Adam steps: 5.36x in two runs on one box against 5.09x and 5.34x at 30000
+GS_TRAIN_STEPS = 120000    # Adam steps: 10.6x on one box against 9.3x at 60000 (35 s of training)
 WORKLOAD = "uneven-ensembles-1024"
 
 
