@@ -418,7 +418,7 @@ def _fptr(a):
 
 
 class MLP:
-    """The warm-start network (bec_mlp_*): tanh MLP, BF16 tensor-core GEMMs, FP32 accumulation."""
+    """The warm-start network (bec_mlp_*): tanh MLP, tensor-core GEMMs on split BF16 operands, FP32 accumulation."""
 
     def __init__(self, widths, seed=0):
         self.widths = [int(w) for w in widths]

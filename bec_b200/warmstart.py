@@ -13,8 +13,9 @@ Pipeline, all on the GPU through the C ABI:
      method of snapshots); it is installed on the device
      (bec_warmstart_set_basis) and every ground state is reduced to its 64
      least-squares coefficients (bec_ground_state_coeffs);
-  3. train the MLP 6 -> 256 -> 256 -> 256 -> 64 (BF16 tensor-core GEMMs, FP32
-     accumulation, Adam) to map normalised parameters to normalised coefficients;
+  3. train the MLP 6 -> 256 -> 256 -> 256 -> 64 (tensor-core GEMMs on split BF16
+     operands, FP32 accumulation, Adam) to map normalised parameters to normalised
+     coefficients;
   4. on held-out parameter sets, run the ground-state loop from Thomas-Fermi
      (cold) and from the network's prediction (warm) with the same stopping rule,
      and compare iterations and device seconds (warm: synthesis and loop, plus the

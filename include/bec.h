@@ -405,8 +405,9 @@ bec_status bec_profile_steps(bec_ctx *ctx, int32_t n_steps, int32_t max_classes,
 
 /*
  * A multilayer perceptron Y = act(X W^T + b) per layer (tanh on hidden layers,
- * identity on the last), trained and evaluated on the GPU with BF16
- * tensor-core GEMMs accumulating in FP32. No counterpart in the reference: it
+ * identity on the last), trained and evaluated on the GPU with tensor-core
+ * GEMMs on split BF16 operands (x = hi + lo, about 16 significant bits)
+ * accumulating in FP32. No counterpart in the reference: it
  * predicts the coefficients of a correction to the Thomas-Fermi profile that
  * seeds bec_ground_state_batch (warm_start), which alone decides convergence.
  * widths has n_layers + 1 entries (inputs, hidden..., outputs). Host parameter
