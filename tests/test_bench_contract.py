@@ -34,6 +34,24 @@ def test_reference_arm_line():
     assert d["e2e"] == {"value": d["value"], "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
+def test_reference_arm_under_torchrun_prints_one_line():
+    """Launched like the multi-GPU bench (torchrun, two ranks, gloo here), the reference arm runs on rank 0
+    alone: exactly one JSON line, every rank exits 0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--n-traj", "8",
+                        "--cpu-seconds", "1"], capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
 def test_baseline_samples_keep_the_batch_mix():
     """The CPU and plain-FP64 baseline samples hold every grid class in the batch's proportion (largest
     remainders), so their traj-steps/s compare with the batch's."""
