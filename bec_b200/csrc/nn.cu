@@ -277,12 +277,14 @@ __global__ void k_colsum(const float *dz, float *db, int R, int Cn)
     db[c] = s;
 }
 
-// dY = 2 (y - t) / (B * out) over the first `valid` rows (padding rows get 0); loss partials
-__global__ void k_mse(const float *y, const float *tgt, float *dy, int rows, int valid, int cols, float *loss)
+// dY = 2 (y - t) / (B * out) over the first `valid` rows (padding rows get 0), out = the caller's output width
+// (real_cols; the padding columns of y and t are zero); loss partials
+__global__ void k_mse(const float *y, const float *tgt, float *dy, int rows, int valid, int cols, int real_cols,
+                      float *loss)
 {
     const size_t n = (size_t)rows * cols;
     float l = 0.0f;
-    const float s = 2.0f / ((float)valid * cols);
+    const float s = 2.0f / ((float)valid * real_cols);
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int r = (int)(i / cols);
         const float d = (r < valid) ? y[i] - tgt[i] : 0.0f;
@@ -290,7 +292,7 @@ __global__ void k_mse(const float *y, const float *tgt, float *dy, int rows, int
         l += d * d;
     }
     for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l / ((float)valid * cols));
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l / ((float)valid * real_cols));
 }
 
 __global__ void k_adam(float *w, float *m, float *v, const float *g, size_t n, float lr, float b1, float b2, float eps,
@@ -439,7 +441,8 @@ void mlp_backward_dev(bec_mlp *m, int rows, int valid)
     cudaStream_t s = m->s;
     const int outw = m->w[m->L];
     cudaMemsetAsync(m->loss, 0, sizeof(float), s);
-    k_mse<<<grid_for((size_t)rows * outw), 256, 0, s>>>(m->y[m->L], m->tgt, m->dy, rows, valid, outw, m->loss);
+    k_mse<<<grid_for((size_t)rows * outw), 256, 0, s>>>(m->y[m->L], m->tgt, m->dy, rows, valid, outw,
+                                                        m->w_real[m->L], m->loss);
     g_launches++;
     for (int l = m->L - 1; l >= 0; --l) {
         const int in = m->w[l], out = m->w[l + 1];

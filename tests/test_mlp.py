@@ -97,6 +97,26 @@ def test_gpu_forward_and_gradients_match_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("widths,batch", [([5, 70, 130, 3], 100), ([6, 256, 64], 64), ([3, 40, 40, 40, 1], 320)])
+def test_gpu_split_gemm_padded_shapes_match_oracle(widths, batch):
+    """Widths that are not multiples of 64 (zero-padded on the device) and batches whose last row tile is 64
+    rows (the GEMM's zero-filled A rows): outputs and gradients against the split-mode oracle."""
+    from bec_b200.engine import MLP
+    x, t = _data(batch, seed=11, widths=widths)
+    p = _params(widths, seed=4)
+    net = MLP(widths, seed=0)
+    net.set_params(p)
+    y = net.forward(x)
+    y_o = M.forward(p, widths, x, arith="split")[-1]
+    assert y.shape == y_o.shape
+    assert np.abs(y - y_o).max() < 1e-4 * np.abs(y_o).max()
+    loss, g = net.gradients(x, t)
+    loss_o, g_o = M.loss_and_grads(p, widths, x, t, arith="split")
+    assert loss == pytest.approx(loss_o, rel=1e-4)
+    assert np.linalg.norm(g - g_o) < 1e-4 * np.linalg.norm(g_o)
+
+
+@pytest.mark.gpu
 def test_gpu_training_reduces_loss():
     from bec_b200.engine import MLP
     x, t = _data(1024, seed=5)
