@@ -172,6 +172,45 @@ def test_uneven_batch_fp32():
             assert rel_state_err(eng.get_state(g, t), e.get_state(t)) < FP32_STATE_SHORT
 
 
+UNUSUAL_GRIDS = [
+    rb87_params(N=20000, grid=(16, 8, 64), ne=2, noise=True, seed=21, fy=70.0),      # nx != ny: generic plane pass
+    rb87_params(N=15000, grid=(8, 8, 32), ne=2, noise=True, seed=22),                # nz = 32: generic z pass
+    rb87_params(N=10000, grid=(4, 4, 512), ne=1, noise=True, seed=23, fz=6.0),       # nz = 512, 4 x 4 planes
+    rb87_params(N=30000, grid=(64, 32, 16), ne=1, noise=True, seed=24, fy=60.0, fz=40.0),  # the largest plane
+    rb87_params(N=25000, grid=(128, 1, 32), ne=2, noise=True, seed=25, fy=50.0),     # a wide 2D slice
+]
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_uneven_batch_unusual_grids(path):
+    """Grid shapes off the register-resident passes (nx != ny, nz of 32 and 512, a 64 x 32 plane, a 128-wide
+    slice), all in one context: states and moments against the oracle after 40 steps with noise and losses."""
+    groups = UNUSUAL_GRIDS
+    eng = Engine(groups, path=path)
+    ens = []
+    for g, p in enumerate(groups):
+        gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=200)
+        eng.init_group(g, gs)
+        e = O.OracleEnsemble(p)
+        e.init(gs)
+        e.start_evolution()
+        ens.append(e)
+    eng.start_evolution()
+    mom = eng.run(40, sample_every=20)
+    for e in ens:
+        e.evolve(40)
+    worst_m, worst_s = 0.0, 0.0
+    for g, (p, e) in enumerate(zip(groups, ens)):
+        err = max(moments_rel_err(mom[-1, g], e.moments()))
+        se = max(rel_state_err(eng.get_state(g, t), e.get_state(t)) for t in range(p.ne))
+        worst_m, worst_s = max(worst_m, err), max(worst_s, se)
+        if path == BEC_PATH_FP64_PLAIN:
+            assert err < FP64_TOL and se < FP64_TOL, (g, err, se)
+        else:
+            assert err < FP32_MOM and se < FP32_STATE_SHORT, (g, err, se)
+    record(f"unusual_grids_{'fp64' if path == BEC_PATH_FP64_PLAIN else 'fp32'}", moments=worst_m, state=worst_s)
+
+
 # ------------------------------------------------------------------ schedule, pulses, observables
 @pytest.mark.parametrize("path", PATHS)
 def test_run_with_pi_pulse_and_axial(path):
