@@ -323,11 +323,17 @@ def gs_warmstart_leg(n_train, n_eval, tol, ref_tol):
         }
 
     accurate = leg(tol)
+    # the basis's own limit: warm starts from the held-out sets' converged coefficients (a diagnostic beside the
+    # network's warm start, not a product path)
+    bound = W.ground_states(ev, coef_in=ref["coef"], basis=basis, tol=tol, check_every=20, max_steps=40000)
     return {
         "workload": f"32x32x256 warm-start ground states, {n_train} training / {n_eval} held-out parameter sets",
         "unit": "s (device time of the held-out batch; warm includes the network's inference)",
         **accurate,
         "reference_rule": leg(ref_tol),
+        "projection_bound": {"note": "warm starts from the held-out sets' own converged coefficients, accurate rule",
+                             "warm_s": bound["seconds"], "warm_steps_mean": float(bound["steps"].mean()),
+                             "speedup_s": accurate["cold_s"] / max(bound["seconds"], 1e-12)},
         "mu_star": f"each held-out set run on to |d mu|/mu < 1e-10 and residual < 1e-9 or 40000 steps "
                    f"({float(ref['steps'].mean()):.0f} steps mean); the FP32 fixed point lies 3e-7 to 4e-7 from "
                    "the FP64 one",
