@@ -59,6 +59,24 @@ def test_batched_fixed_steps_match_oracle():
     assert worst < 2e-5
 
 
+def test_batched_every_supported_shape_matches_oracle():
+    """Every grid the batched loop takes (square 8, 16 and 32 planes by nz = 64, 128 and 256), nine classes in
+    one context: 100 fixed steps against the oracle."""
+    groups = [rb87_params(N=20000 + 5000 * k, grid=(n, n, nz), fz=11.0 + k)
+              for k, (n, nz) in enumerate((n, nz) for n in (8, 16, 32) for nz in (64, 128, 256))]
+    eng = Engine(groups, path=BEC_PATH_FP32_BATCHED)
+    outs, reps = batch_gs(eng, list(range(len(groups))), BEC_GS_FIXED_STEPS, 100)
+    worst = 0.0
+    for g, p in enumerate(groups):
+        psi_o, rep_o = O.ground_state(p, mode=BEC_GS_FIXED_STEPS, max_steps=100)
+        err = rel_state_err(outs[g], psi_o)
+        worst = max(worst, err)
+        assert reps[g].steps == 100
+        assert reps[g].mu == pytest.approx(rep_o.mu, rel=1e-6), (p.nvx, p.nvz)
+        assert err < 2e-5, (p.nvx, p.nvz, err)
+    record("gs_batched_every_shape_fixed100", state_err=worst)
+
+
 def test_batched_mu_rule_matches_oracle():
     sel = [0, 2]
     eng = Engine(GROUPS, path=BEC_PATH_FP32_BATCHED)
