@@ -172,6 +172,51 @@ def test_uneven_batch_fp32():
             assert rel_state_err(eng.get_state(g, t), e.get_state(t)) < FP32_STATE_SHORT
 
 
+# the register-resident shapes the other tests leave out (8, 16, 32 planes by nz = 64, 128, 256)
+FAST_SHAPES = [
+    rb87_params(N=15000, grid=(8, 8, 128), ne=2, noise=True, seed=31),
+    rb87_params(N=20000, grid=(8, 8, 256), ne=2, noise=True, seed=32, fz=8.0),
+    rb87_params(N=30000, grid=(16, 16, 256), ne=2, noise=True, seed=33),
+    rb87_params(N=40000, grid=(32, 32, 64), ne=2, noise=True, seed=34, fz=30.0),
+    rb87_params(N=50000, grid=(32, 32, 128), ne=2, noise=True, seed=35),
+]
+
+
+@pytest.fixture(scope="module")
+def fast_shape_oracle():
+    gss, moms, states = [], [], []
+    for p in FAST_SHAPES:
+        gs, _ = O.ground_state(copy_params(p, ne=1), max_steps=200)
+        e = O.OracleEnsemble(p)
+        e.init(gs)
+        e.start_evolution()
+        e.evolve(40)
+        gss.append(gs)
+        moms.append(e.moments())
+        states.append([e.get_state(t) for t in range(p.ne)])
+    return gss, moms, states
+
+
+@pytest.mark.parametrize("plan", ["unfused", "unfused-tma"])
+def test_register_shapes_off_the_workload(monkeypatch, fast_shape_oracle, plan):
+    """The register-resident plane and pencil passes (register or TMA pencils) on the shapes the workload does
+    not use, one context: states and moments against the oracle after 40 steps with noise and losses."""
+    monkeypatch.setenv("BEC_STEP_PLAN", plan)
+    gss, moms, states = fast_shape_oracle
+    eng = Engine(FAST_SHAPES, path=BEC_PATH_FP32_BATCHED)
+    for g, gs in enumerate(gss):
+        eng.init_group(g, gs)
+    eng.start_evolution()
+    mom = eng.run(40, sample_every=20)
+    worst_m, worst_s = 0.0, 0.0
+    for g, p in enumerate(FAST_SHAPES):
+        err = max(moments_rel_err(mom[-1, g], moms[g]))
+        se = max(rel_state_err(eng.get_state(g, t), states[g][t]) for t in range(p.ne))
+        worst_m, worst_s = max(worst_m, err), max(worst_s, se)
+        assert err < FP32_MOM and se < FP32_STATE_SHORT, ((p.nvx, p.nvz), err, se)
+    record(f"register_shapes_{plan}", moments=worst_m, state=worst_s)
+
+
 UNUSUAL_GRIDS = [
     rb87_params(N=20000, grid=(16, 8, 64), ne=2, noise=True, seed=21, fy=70.0),      # nx != ny: generic plane pass
     rb87_params(N=15000, grid=(8, 8, 32), ne=2, noise=True, seed=22),                # nz = 32: generic z pass
