@@ -17,6 +17,12 @@
  * Defined here (no reference code exists; the product follows the same
  * definitions): Philox4x32-10 noise, the Wigner loss-noise increment, the 2D
  * transverse renormalisation, the mu/energy/residual measures.
+ *
+ * Pinned (the reference itself cannot be built here) by known-answer tests in
+ * tests/test_oracle.py (the published Random123 Philox vectors among them) and
+ * by the reference's own stored GPU output: with the loss rates written in its
+ * parameter set (wigner.cpp:74-76) this oracle follows data/gpu_sp_30k.yaml
+ * within 0.019 in visibility over all of its 0.6 s (tests/test_golden.py).
  */
 #include "bec_oracle.h"
 
